@@ -1,0 +1,176 @@
+/*
+ * pfem_b200.h -- C ABI of the B200 finite-strain F-bar J2 plasticity path.
+ *
+ * Drop-in for the per-Newton-iteration path of vinaysrao1/plasticity,
+ * lagrangian/ (Julia).  A Julia shim binds these symbols with `ccall` (see
+ * INTEGRATION.md); the Python package `plasticity_b200` binds them with ctypes.
+ *
+ * Conventions (same as the reference):
+ *   - node coordinates: 3 x nn, column-major (nodes[3*n + d]), Mesh.jl:17-22
+ *   - element connectivity: 8 x ne, column-major, 1-based Int64, VTK Hex8 order
+ *   - dof(n, c) = 3(n-1) + c (1-based), Mesh.jl:111; U is node-major
+ *   - per-Gauss-point arrays: 6 x ngp column-major, gp = 8(e-1) + g, Mesh.jl:124-130
+ *   - Voigt [xx,yy,zz,xy,yz,zx]; strain engineering shear, stress physical shear
+ *   - sparsity exported as 1-based CSC (colptr/rowval), Assembly.jl:99-148
+ *
+ * Ownership: host buffers are read/written only during a call.  The library
+ * owns one device context per pfem_ctx (device memory + one CUDA stream);
+ * calls on one context are synchronous and must not run concurrently.
+ * Errors: every call returns a pfem_status; no C++ exception crosses the ABI.
+ * There is no CPU fallback: every call that computes runs on the GPU and
+ * returns PFEM_ERR_CUDA when no usable device is present.
+ */
+#ifndef PFEM_B200_H
+#define PFEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pfem_ctx pfem_ctx;
+
+enum pfem_status {
+  PFEM_OK = 0,
+  PFEM_ERR_BAD_ARG = -1,          /* ArgumentError guards, Materials.jl:90-103 */
+  PFEM_ERR_CUDA = -2,             /* CUDA runtime failure (message in pfem_last_error) */
+  PFEM_ERR_INVERTED_ELEMENT = -3, /* ElementInversionError, FiniteStrain.jl:42-52 */
+  PFEM_ERR_LINSOLVE = -4,         /* Krylov solve missed its tolerance, Solver.jl:268-287 */
+  PFEM_ERR_NOT_CONVERGED = -5,    /* Newton non-convergence, Solver.jl:463-467 */
+  PFEM_ERR_STATE = -6             /* call made in the wrong state (e.g. no tangent yet) */
+};
+
+/* Element kinds, FiniteStrain.jl:62-65 (Hex8Finite / Hex8FiniteFbar). */
+enum pfem_kind { PFEM_HEX8_FINITE = 1, PFEM_HEX8_FINITE_FBAR = 2 };
+/* Tangent / inner-solve precision: FP64 throughout, or FP32 tangent + FP32
+ * Krylov/AMG inside the FP64 Newton residual loop. */
+enum pfem_precision { PFEM_FP64 = 0, PFEM_MIXED = 1 };
+/* Newton predictor for each load step: previous converged U (the reference,
+ * Solver.jl:321-323), linear extrapolation of the last two increments, or the
+ * learned per-node MLP with extrapolation as fallback. */
+enum pfem_predictor { PFEM_PRED_PREVIOUS = 0, PFEM_PRED_EXTRAPOLATE = 1, PFEM_PRED_LEARNED = 2 };
+enum pfem_krylov { PFEM_KRYLOV_CG = 0, PFEM_KRYLOV_BICGSTAB = 1 };
+
+/* J2Material(; E, nu, sigy0, Hiso, Hkin), Materials.jl:82-108.  This path
+ * supports linear isotropic hardening; Hkin must be 0. */
+typedef struct pfem_material {
+  double E, nu, sigy0, Hiso, Hkin;
+} pfem_material;
+
+/* Keyword arguments of solve!, Solver.jl:419-422, and LinearSolveState,
+ * Solver.jl:103-108. */
+typedef struct pfem_solve_opts {
+  int32_t nsteps;        /* load steps, lambda = n/nsteps */
+  int32_t maxiter;       /* Newton iterations per load step */
+  double tol;            /* Newton relative residual tolerance */
+  int32_t precision;     /* pfem_precision */
+  int32_t krylov;        /* pfem_krylov */
+  double lin_rtol;       /* > 0: fixed Krylov rtol; <= 0: Eisenstat-Walker forcing */
+  double eta_min, eta_max, ew_gamma, ew_alpha;
+  int32_t krylov_itmax;  /* cg_itmax */
+  int32_t predictor;     /* pfem_predictor */
+  int32_t amg_rebuild;   /* 0: once per load step (reference policy); 1: every Newton iteration */
+  int32_t cheb_degree;   /* Chebyshev smoother degree */
+  int32_t verbose;
+  int32_t line_search;   /* 0: full Newton steps (the reference); 1: backtrack (halving, at
+                            most 8 times) until the FP64 residual norm decreases -- the
+                            accepted trial assembly is the next iterate, so a full step
+                            costs nothing extra */
+} pfem_solve_opts;
+
+typedef struct pfem_solve_result {
+  int32_t converged;
+  int32_t steps_done;
+  int32_t newton_iters_total;   /* sum of SolveResult.iters (each counts the final check) */
+  int32_t krylov_iters_total;
+  int32_t predictor_learned_used; /* load steps where the learned guess won */
+  double time_total_ms;
+  double time_assembly_ms;      /* element kernels incl. scatter, device time */
+  double time_amg_setup_ms;
+  double time_krylov_ms;
+  double time_predictor_ms;
+} pfem_solve_result;
+
+void pfem_default_opts(pfem_solve_opts* o);
+
+/* Model(mesh, material; element=:finite_fbar), Model.jl:63-75, plus
+ * build_sparsity / element_colors (Assembly.jl:99-206) and
+ * precompute_cache (Elements.jl:291-308).  sigy0_e: optional per-element
+ * initial yield stress (ne values) replacing mat->sigy0.  device < 0 builds a
+ * topology-only context (pattern and colors; compute calls return
+ * PFEM_ERR_STATE) that needs no GPU. */
+int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* elements,
+                int64_t ne, int32_t kind, const pfem_material* mat, const double* sigy0_e,
+                int32_t device);
+void pfem_destroy(pfem_ctx* ctx);
+const char* pfem_last_error(const pfem_ctx* ctx);
+/* ElementInversionError fields (e, g 1-based; J = det Fbar), FiniteStrain.jl:42-46. */
+int pfem_inversion_info(const pfem_ctx* ctx, int64_t* e, int32_t* g, double* J);
+
+/* SparsityPattern.K structure (Assembly.jl:99-148): nnz, then 1-based
+ * colptr (3nn+1) / rowval (nnz) when the pointers are non-null. */
+int pfem_pattern(const pfem_ctx* ctx, int64_t* nnz, int64_t* colptr, int64_t* rowval);
+/* element_colors (Assembly.jl:172-206): count and 0-based color per element. */
+int pfem_colors(const pfem_ctx* ctx, int32_t* ncolors, int64_t* color_of_element);
+
+/* fix!/prescribe!/load! accumulators frozen by _freeze_bcs (Solver.jl:192-218):
+ * Dirichlet dofs (1-based, duplicates: last wins), values, ramp flags; Neumann
+ * dofs and nodal forces (ramped by lambda). */
+int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
+                 const uint8_t* dir_ramp, int64_t ndir, const int64_t* neu_dofs,
+                 const double* neu_vals, int64_t nneu);
+
+/* reset! (Model.jl:157-162): U = 0, Cp^-1 = I, alpha = 0, eps_p = 0. */
+int pfem_reset(pfem_ctx* ctx);
+
+/* assemble! (Assembly.jl:238-257) at displacement U (host, ndof) against the
+ * committed state: writes F_int into R (ndof) and, if Kvals is non-null, the
+ * tangent values in the order of the exported pattern read as CSR (row r,
+ * columns rowval[colptr[r]..]); tau (6 x ngp) / flags (ngp) of the evaluation.
+ * commit != 0 advances the committed state (Elements.jl:483-491).
+ * precision selects the tangent storage (FP64 or FP32). */
+int pfem_assemble(pfem_ctx* ctx, const double* U, int32_t commit, int32_t precision, double* R,
+                  double* Kvals, double* tau, uint8_t* flags);
+
+/* newton! (Solver.jl:317-389) for one load step at load factor lambda from
+ * the context's current U and committed state, followed by the commit pass
+ * (Solver.jl:470-471) when it converges.  res_hist / krylov_hist (capacity
+ * maxiter) receive the residual norms and Krylov iteration counts. */
+int pfem_newton(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, int32_t* iters,
+                double* res_hist, int32_t* krylov_hist);
+
+/* solve! (Solver.jl:419-475): reset, load loop, Newton, commit.
+ * iters_per_step (nsteps), residuals (nsteps x maxiter, row per step) and
+ * krylov_per_iter (nsteps x maxiter) may be null. */
+int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res,
+               int32_t* iters_per_step, double* residuals, int32_t* krylov_per_iter);
+
+/* _linear_solve! (Solver.jl:235-290) on the tangent left by the last Newton
+ * iteration (Dirichlet rows imposed): x = K^-1 b to relative tolerance rtol. */
+int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, int32_t rebuild_pc,
+                      const pfem_solve_opts* o, int32_t* niter);
+
+/* Read-out: nodal_displacements / gauss_kirchhoff / equivalent_plastic_strain /
+ * Cp^-1 / eps_p / last elastic-plastic flags (Model.jl:169-232).  Null pointers
+ * are skipped.  Per-GP arrays are 6 x ngp column-major. */
+int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, double* cpi,
+                   double* epsp, uint8_t* flags);
+/* Overwrite the committed per-GP state (6 x ngp Cp^-1, ngp alpha, optional
+ * 6 x ngp eps_p; null pointers keep the current values). */
+int pfem_set_state(pfem_ctx* ctx, const double* cpi, const double* alpha, const double* epsp);
+/* Overwrite U (host ndof) -- e.g. to evaluate a predictor guess. */
+int pfem_set_displacement(pfem_ctx* ctx, const double* U);
+/* gauss_stress (Model.jl:188-208): Cauchy = tau / det F_gp (standard F). */
+int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma);
+
+/* Device timing of one hot-path kernel family on the resident data, CUDA
+ * events on the context's stream, averaged over reps launches.
+ * what: 0 = element kernels of one full assembly (all colors, FP64 tangent),
+ *       1 = same with the FP32 tangent, 2 = level-0 SpMV FP32, 3 = SpMV FP64. */
+int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFEM_B200_H */

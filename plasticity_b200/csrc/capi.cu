@@ -1,0 +1,1621 @@
+// capi.cu -- the extern "C" boundary (include/pfem_b200.h): context set-up,
+// host-side one-time topology work, the device Newton load loop, the Krylov
+// solvers and the aggregation AMG they use.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "linalg.cuh"
+#include "mlp.cuh"
+
+using namespace pfem;
+
+static thread_local std::string g_cuda_err;
+void pfem_set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what,
+           file, line);
+  g_cuda_err = buf;
+}
+
+namespace {
+
+template <typename T>
+struct KrylovWork {
+  long long n = 0;
+  T *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+  T *rh = nullptr, *v = nullptr, *s = nullptr, *t = nullptr, *ph = nullptr, *sh = nullptr;
+  T* sc = nullptr;    // device scalars
+  T* part = nullptr;  // reduction partials
+  T* b = nullptr;
+};
+
+struct HostLevel {
+  int nbrow = 0, bs = 0;
+  std::vector<int> rowptr, col;
+  int nagg = 0;
+  std::vector<int> agg, aptr, amem, f2c;
+  std::vector<double> T;  // nbrow*bs*6
+};
+
+}  // namespace
+
+struct pfem_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  long long nn = 0, ne = 0, ngp = 0, ndof = 0;
+  int kind = PFEM_HEX8_FINITE_FBAR;
+  MatParams mat{};
+  std::string err;
+  std::vector<void*> allocs;
+
+  // host topology
+  std::vector<double> X;        // nn*3
+  std::vector<int> elem;        // ne*8, 0-based
+  std::vector<int> browptr, bcol;
+  long long nnzb = 0;
+  int ncolors_ref = 0;
+  std::vector<int64_t> color_ref;
+  std::vector<int> color_ptr;   // device coloring, CSR over colors
+  // device topology / state
+  double* dX = nullptr;
+  int* dElem = nullptr;
+  uint8_t* dRank = nullptr;
+  int* dBrowptr = nullptr;
+  int* dBcol = nullptr;
+  double* dSigy = nullptr;
+  int* dColorList = nullptr;
+  int* dAllElems = nullptr;
+  double *dCpi = nullptr, *dAlpha = nullptr, *dEpsp = nullptr, *dTau = nullptr;
+  uint8_t* dFlags = nullptr;
+  double *dU = nullptr, *dR = nullptr, *dDg = nullptr, *dUprev = nullptr, *dUprev2 = nullptr;
+  double *dUtmp = nullptr, *dScal = nullptr, *dPart = nullptr;
+  double* dK64 = nullptr;
+  float* dK32 = nullptr;
+  DevStatus* dStatus = nullptr;
+  // boundary conditions
+  bool bcs_set = false;
+  BcDev bc;
+  double fn_norm = 0.0;
+  // solver
+  std::vector<HostLevel> hl;
+  bool amg_struct = false;
+  Amg<float> amg32;
+  Amg<double> amg64;
+  KrylovWork<float> kw32;
+  KrylovWork<double> kw64;
+  int tangent_prec = -1;  // precision of the last imposed tangent
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // learned predictor
+  pfem::MlpState mlp;
+  int steps_taken = 0;
+  double lam_prev = 0.0, lam_prev2 = 0.0;
+};
+
+namespace {
+
+int fail(pfem_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+int cuda_fail(pfem_ctx* c) {
+  if (c) c->err = g_cuda_err;
+  return PFEM_ERR_CUDA;
+}
+#define CK(expr)                                              \
+  do {                                                        \
+    cudaError_t e__ = (expr);                                 \
+    if (e__ != cudaSuccess) {                                 \
+      pfem_set_cuda_error(e__, #expr, __FILE__, __LINE__);    \
+      return cuda_fail(ctx);                                  \
+    }                                                         \
+  } while (0)
+#define CKL()                                                 \
+  do {                                                        \
+    cudaError_t e__ = cudaGetLastError();                     \
+    if (e__ != cudaSuccess) {                                 \
+      pfem_set_cuda_error(e__, "kernel launch", __FILE__, __LINE__); \
+      return cuda_fail(ctx);                                  \
+    }                                                         \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(pfem_ctx* ctx, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e == cudaSuccess) ctx->allocs.push_back((void*)*p);
+  return e;
+}
+template <typename T>
+cudaError_t upload(pfem_ctx* ctx, T** p, const std::vector<T>& h) {
+  cudaError_t e = dalloc(ctx, p, h.size());
+  if (e != cudaSuccess) return e;
+  if (!h.empty()) e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+template <class Fn>
+void par_for(long long n, Fn fn) {
+  const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 20000 || nt == 1) {
+    for (long long i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long long chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    const long long b = t * chunk, e = std::min(n, b + chunk);
+    if (b >= e) break;
+    th.emplace_back([=, &fn]() {
+      for (long long i = b; i < e; ++i) fn(i);
+    });
+  }
+  for (auto& t : th) t.join();
+}
+
+// element_colors reference rule (Assembly.jl:172-206): parity colors when
+// the node coordinates form an axis-aligned structured box, else one color.
+int reference_colors(const std::vector<double>& X, long long nn, long long ne,
+                     std::vector<int64_t>& color) {
+  color.assign(ne, 0);
+  if (ne == 0) return 0;
+  long long dims[3];
+  for (int d = 0; d < 3; ++d) {
+    std::vector<double> v(nn);
+    for (long long n = 0; n < nn; ++n) v[n] = std::round(X[n * 3 + d] * 1e12) / 1e12;
+    std::sort(v.begin(), v.end());
+    dims[d] = (long long)(std::unique(v.begin(), v.end()) - v.begin()) - 1;
+  }
+  const long long nx = dims[0], ny = dims[1], nz = dims[2];
+  if (!(nx >= 1 && ny >= 1 && nz >= 1 && nx * ny * nz == ne && (nx + 1) * (ny + 1) * (nz + 1) == nn))
+    return 1;
+  int raw[8] = {0};
+  std::vector<int> c8(ne);
+  long long e = 0;
+  for (long long k = 0; k < nz; ++k)
+    for (long long j = 0; j < ny; ++j)
+      for (long long i = 0; i < nx; ++i) {
+        const int c = (int)((i & 1) + 2 * (j & 1) + 4 * (k & 1));
+        c8[e++] = c;
+        raw[c]++;
+      }
+  int remap[8], nc = 0;
+  for (int c = 0; c < 8; ++c) remap[c] = raw[c] ? nc++ : -1;
+  for (long long q = 0; q < ne; ++q) color[q] = remap[c8[q]];
+  return nc;
+}
+
+// Greedy first-fit element coloring on the shared-node graph (used when the
+// reference rule gives a single color, i.e. on perturbed meshes).
+int greedy_colors(const std::vector<int>& elem, long long nn, long long ne, std::vector<int>& col) {
+  std::vector<int> nptr(nn + 1, 0);
+  for (long long e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) nptr[elem[e * 8 + a] + 1]++;
+  for (long long n = 0; n < nn; ++n) nptr[n + 1] += nptr[n];
+  std::vector<int> nel(nptr[nn]);
+  std::vector<int> fill(nptr.begin(), nptr.end() - 1);
+  for (long long e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) nel[fill[elem[e * 8 + a]]++] = (int)e;
+  col.assign(ne, -1);
+  int nc = 0;
+  for (long long e = 0; e < ne; ++e) {
+    uint64_t used = 0;
+    for (int a = 0; a < 8; ++a) {
+      const int n = elem[e * 8 + a];
+      for (int k = nptr[n]; k < nptr[n + 1]; ++k) {
+        const int o = nel[k];
+        if (col[o] >= 0 && col[o] < 64) used |= (1ull << col[o]);
+      }
+    }
+    int c = 0;
+    while (c < 64 && (used >> c) & 1ull) ++c;
+    col[e] = c;
+    nc = std::max(nc, c + 1);
+  }
+  return nc;
+}
+
+// Greedy aggregation on a block graph: phase 1 roots whose neighbourhood is
+// untouched, phase 2 attaches leftovers to an adjacent aggregate, phase 3
+// groups whatever remains with its unaggregated neighbours.
+int aggregate(int nb, const std::vector<int>& rp, const std::vector<int>& cl, std::vector<int>& agg) {
+  agg.assign(nb, -1);
+  int na = 0;
+  for (int n = 0; n < nb; ++n) {
+    if (agg[n] >= 0) continue;
+    bool free_ = true;
+    for (int k = rp[n]; k < rp[n + 1] && free_; ++k)
+      if (agg[cl[k]] >= 0) free_ = false;
+    if (!free_) continue;
+    for (int k = rp[n]; k < rp[n + 1]; ++k) agg[cl[k]] = na;
+    agg[n] = na;
+    ++na;
+  }
+  std::vector<int> agg1 = agg;
+  for (int n = 0; n < nb; ++n) {
+    if (agg[n] >= 0) continue;
+    for (int k = rp[n]; k < rp[n + 1]; ++k)
+      if (agg1[cl[k]] >= 0) { agg[n] = agg1[cl[k]]; break; }
+  }
+  for (int n = 0; n < nb; ++n) {
+    if (agg[n] >= 0) continue;
+    agg[n] = na;
+    for (int k = rp[n]; k < rp[n + 1]; ++k)
+      if (agg[cl[k]] < 0) agg[cl[k]] = na;
+    ++na;
+  }
+  return na;
+}
+
+// Thin QR (modified Gram-Schmidt, two passes) of an m x 6 block, row-major.
+void mgs_qr(int m, std::vector<double>& A, double R[36]) {
+  std::memset(R, 0, 36 * sizeof(double));
+  double n0[6];
+  for (int c = 0; c < 6; ++c) {
+    double s = 0;
+    for (int i = 0; i < m; ++i) s += A[i * 6 + c] * A[i * 6 + c];
+    n0[c] = std::sqrt(s);
+  }
+  for (int c = 0; c < 6; ++c) {
+    for (int pass = 0; pass < 2; ++pass)
+      for (int k = 0; k < c; ++k) {
+        double s = 0;
+        for (int i = 0; i < m; ++i) s += A[i * 6 + k] * A[i * 6 + c];
+        R[k * 6 + c] += s;
+        for (int i = 0; i < m; ++i) A[i * 6 + c] -= s * A[i * 6 + k];
+      }
+    double s = 0;
+    for (int i = 0; i < m; ++i) s += A[i * 6 + c] * A[i * 6 + c];
+    s = std::sqrt(s);
+    if (s > 1e-10 * std::max(n0[c], 1e-300)) {
+      R[c * 6 + c] = s;
+      for (int i = 0; i < m; ++i) A[i * 6 + c] /= s;
+    } else {
+      R[c * 6 + c] = 0.0;
+      for (int i = 0; i < m; ++i) A[i * 6 + c] = 0.0;
+    }
+  }
+}
+
+// Host side of the AMG hierarchy: aggregates, tentative prolongators from the
+// six rigid-body modes (Solver.jl:117-129), coarse patterns, fine->coarse maps.
+void build_amg_structure(pfem_ctx* c) {
+  c->hl.clear();
+  HostLevel L0;
+  L0.nbrow = (int)c->nn;
+  L0.bs = 3;
+  L0.rowptr = c->browptr;
+  L0.col = c->bcol;
+  std::vector<double> B((size_t)c->nn * 3 * 6, 0.0);  // rows (node,comp) x 6
+  bool first = true;
+  HostLevel cur = std::move(L0);
+  for (int lev = 0; lev < 10; ++lev) {
+    const int nb = cur.nbrow, bs = cur.bs;
+    if ((long long)nb * bs <= 600 && !first) break;
+    cur.nagg = aggregate(nb, cur.rowptr, cur.col, cur.agg);
+    if (cur.nagg >= nb || (long long)cur.nagg * 6 >= (long long)nb * bs) break;
+    cur.aptr.assign(cur.nagg + 1, 0);
+    for (int n = 0; n < nb; ++n) cur.aptr[cur.agg[n] + 1]++;
+    for (int a = 0; a < cur.nagg; ++a) cur.aptr[a + 1] += cur.aptr[a];
+    cur.amem.assign(nb, 0);
+    {
+      std::vector<int> f(cur.aptr.begin(), cur.aptr.end() - 1);
+      for (int n = 0; n < nb; ++n) cur.amem[f[cur.agg[n]]++] = n;
+    }
+    cur.T.assign((size_t)nb * bs * 6, 0.0);
+    std::vector<double> Bc((size_t)cur.nagg * 36, 0.0);
+    for (int a = 0; a < cur.nagg; ++a) {
+      const int m = cur.aptr[a + 1] - cur.aptr[a];
+      std::vector<double> M((size_t)m * bs * 6);
+      if (first) {
+        double cx = 0, cy = 0, cz = 0;
+        for (int k = cur.aptr[a]; k < cur.aptr[a + 1]; ++k) {
+          const int n = cur.amem[k];
+          cx += c->X[n * 3]; cy += c->X[n * 3 + 1]; cz += c->X[n * 3 + 2];
+        }
+        cx /= m; cy /= m; cz /= m;
+        for (int q = 0; q < m; ++q) {
+          const int n = cur.amem[cur.aptr[a] + q];
+          const double x = c->X[n * 3] - cx, y = c->X[n * 3 + 1] - cy, z = c->X[n * 3 + 2] - cz;
+          double* r0 = &M[(q * 3 + 0) * 6];
+          double* r1 = &M[(q * 3 + 1) * 6];
+          double* r2 = &M[(q * 3 + 2) * 6];
+          for (int k = 0; k < 6; ++k) r0[k] = r1[k] = r2[k] = 0.0;
+          r0[0] = 1; r1[1] = 1; r2[2] = 1;
+          r1[3] = -z; r2[3] = y;
+          r0[4] = z; r2[4] = -x;
+          r0[5] = -y; r1[5] = x;
+        }
+      } else {
+        for (int q = 0; q < m; ++q) {
+          const int n = cur.amem[cur.aptr[a] + q];
+          for (int i = 0; i < bs * 6; ++i) M[(size_t)q * bs * 6 + i] = B[(size_t)n * bs * 6 + i];
+        }
+      }
+      double R[36];
+      mgs_qr(m * bs, M, R);
+      for (int q = 0; q < m; ++q) {
+        const int n = cur.amem[cur.aptr[a] + q];
+        for (int i = 0; i < bs * 6; ++i) cur.T[(size_t)n * bs * 6 + i] = M[(size_t)q * bs * 6 + i];
+      }
+      for (int i = 0; i < 36; ++i) Bc[(size_t)a * 36 + i] = R[i];
+    }
+    // coarse pattern + fine->coarse block map
+    std::vector<std::vector<int>> cadj(cur.nagg);
+    for (int n = 0; n < nb; ++n)
+      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) cadj[cur.agg[n]].push_back(cur.agg[cur.col[k]]);
+    HostLevel nxt;
+    nxt.nbrow = cur.nagg;
+    nxt.bs = 6;
+    nxt.rowptr.assign(cur.nagg + 1, 0);
+    for (int a = 0; a < cur.nagg; ++a) {
+      auto& v = cadj[a];
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      nxt.rowptr[a + 1] = nxt.rowptr[a] + (int)v.size();
+    }
+    nxt.col.resize(nxt.rowptr[cur.nagg]);
+    for (int a = 0; a < cur.nagg; ++a) std::copy(cadj[a].begin(), cadj[a].end(), nxt.col.begin() + nxt.rowptr[a]);
+    cur.f2c.resize(cur.rowptr[nb]);
+    for (int n = 0; n < nb; ++n) {
+      const int I = cur.agg[n];
+      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) {
+        const int J = cur.agg[cur.col[k]];
+        const int* b0 = nxt.col.data() + nxt.rowptr[I];
+        const int* b1 = nxt.col.data() + nxt.rowptr[I + 1];
+        cur.f2c[k] = nxt.rowptr[I] + (int)(std::lower_bound(b0, b1, J) - b0);
+      }
+    }
+    c->hl.push_back(std::move(cur));
+    cur = std::move(nxt);
+    B = std::move(Bc);
+    first = false;
+  }
+  c->hl.push_back(std::move(cur));  // coarsest: pattern only
+  c->amg_struct = true;
+}
+
+template <typename T>
+Amg<T>& amg_of(pfem_ctx* c);
+template <>
+Amg<float>& amg_of<float>(pfem_ctx* c) { return c->amg32; }
+template <>
+Amg<double>& amg_of<double>(pfem_ctx* c) { return c->amg64; }
+template <typename T>
+KrylovWork<T>& kw_of(pfem_ctx* c);
+template <>
+KrylovWork<float>& kw_of<float>(pfem_ctx* c) { return c->kw32; }
+template <>
+KrylovWork<double>& kw_of<double>(pfem_ctx* c) { return c->kw64; }
+template <typename T>
+T* K_of(pfem_ctx* c);
+template <>
+float* K_of<float>(pfem_ctx* c) { return c->dK32; }
+template <>
+double* K_of<double>(pfem_ctx* c) { return c->dK64; }
+
+__global__ void hash_fill_kernel(long long n, float* xf, double* xd) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long h = (unsigned long long)i * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29; h *= 0xBF58476D1CE4E5B9ull; h ^= h >> 32;
+    const double v = 0.5 + (double)(h & 0xFFFFFF) / (double)0x1000000;
+    if (xf) xf[i] = (float)v;
+    if (xd) xd[i] = v;
+  }
+}
+template <typename T>
+__global__ void scale_by_inv_kernel(long long n, const T* __restrict__ s, const T* __restrict__ w, T* __restrict__ v) {
+  const T inv = T(1) / *s;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = w[i] * inv;
+}
+template <typename T>
+__global__ void bicg_finish_kernel(T* sc) {
+  sc[2] = sc[0] / sc[4];
+  sc[3] = sc[5] / sc[6];
+  sc[1] = sc[0];
+}
+template <typename T>
+__global__ void bicg_init_kernel(T* sc) {
+  sc[1] = T(1); sc[2] = T(1); sc[3] = T(1);
+}
+
+// Allocate the device side of the hierarchy for precision T (once).
+template <typename T>
+int amg_alloc(pfem_ctx* ctx) {
+  Amg<T>& A = amg_of<T>(ctx);
+  if (!A.lv.empty()) return PFEM_OK;
+  const int L = (int)ctx->hl.size();
+  if (L < 2) return fail(ctx, PFEM_ERR_STATE, "mesh too small to build an aggregation hierarchy");
+  A.lv.resize(L - 1);
+  for (int l = 0; l < L - 1; ++l) {
+    const HostLevel& h = ctx->hl[l];
+    AmgLevel<T>& v = A.lv[l];
+    v.A.nbrow = h.nbrow;
+    v.A.bs = h.bs;
+    v.A.nnzb = h.rowptr[h.nbrow];
+    if (l == 0) {
+      v.A.rowptr = ctx->dBrowptr;
+      v.A.col = ctx->dBcol;
+    } else {
+      CK(upload(ctx, &v.A.rowptr, h.rowptr));
+      CK(upload(ctx, &v.A.col, h.col));
+      CK(dalloc(ctx, &v.A.val, (size_t)v.A.nnzb * h.bs * h.bs));
+    }
+    CK(dalloc(ctx, &v.dinv, (size_t)h.nbrow * h.bs * h.bs));
+    v.nagg = h.nagg;
+    CK(upload(ctx, &v.agg, h.agg));
+    CK(upload(ctx, &v.agg_ptr, h.aptr));
+    CK(upload(ctx, &v.agg_mem, h.amem));
+    CK(upload(ctx, &v.fine2coarse, h.f2c));
+    std::vector<T> Th(h.T.begin(), h.T.end());
+    CK(upload(ctx, &v.T, Th));
+    const size_t n = (size_t)h.nbrow * h.bs;
+    CK(dalloc(ctx, &v.x, n)); CK(dalloc(ctx, &v.b, n)); CK(dalloc(ctx, &v.r, n));
+    CK(dalloc(ctx, &v.d, n)); CK(dalloc(ctx, &v.t, n));
+  }
+  const HostLevel& hc = ctx->hl[L - 1];
+  A.coarse_n = hc.nbrow * hc.bs;
+  CK(dalloc(ctx, &A.coarse_inv, (size_t)A.coarse_n * A.coarse_n));
+  CK(dalloc(ctx, &A.cx, (size_t)A.coarse_n));
+  CK(dalloc(ctx, &A.cb, (size_t)A.coarse_n));
+  return PFEM_OK;
+}
+
+template <typename T>
+int krylov_alloc(pfem_ctx* ctx) {
+  KrylovWork<T>& w = kw_of<T>(ctx);
+  if (w.n == ctx->ndof) return PFEM_OK;
+  const size_t n = ctx->ndof;
+  w.n = ctx->ndof;
+  CK(dalloc(ctx, &w.x, n)); CK(dalloc(ctx, &w.r, n)); CK(dalloc(ctx, &w.z, n));
+  CK(dalloc(ctx, &w.p, n)); CK(dalloc(ctx, &w.q, n)); CK(dalloc(ctx, &w.rh, n));
+  CK(dalloc(ctx, &w.v, n)); CK(dalloc(ctx, &w.s, n)); CK(dalloc(ctx, &w.t, n));
+  CK(dalloc(ctx, &w.ph, n)); CK(dalloc(ctx, &w.sh, n)); CK(dalloc(ctx, &w.b, n));
+  CK(dalloc(ctx, &w.sc, 16)); CK(dalloc(ctx, &w.part, 2048));
+  return PFEM_OK;
+}
+
+// Gauss-Jordan inverse of a dense n x n matrix (row-major, double) with
+// partial pivoting; near-singular pivots are regularised.
+void dense_inverse(int n, std::vector<double>& a, std::vector<double>& inv) {
+  inv.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+  double scl = 0;
+  for (int i = 0; i < n; ++i) scl = std::max(scl, std::fabs(a[(size_t)i * n + i]));
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    double best = std::fabs(a[(size_t)c * n + c]);
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(a[(size_t)r * n + c]) > best) { best = std::fabs(a[(size_t)r * n + c]); piv = r; }
+    if (piv != c)
+      for (int j = 0; j < n; ++j) {
+        std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
+        std::swap(inv[(size_t)c * n + j], inv[(size_t)piv * n + j]);
+      }
+    double pv = a[(size_t)c * n + c];
+    if (std::fabs(pv) < 1e-14 * std::max(scl, 1e-300)) pv = (pv >= 0 ? 1.0 : -1.0) * 1e-14 * std::max(scl, 1e-300);
+    const double ip = 1.0 / pv;
+    for (int j = 0; j < n; ++j) { a[(size_t)c * n + j] *= ip; inv[(size_t)c * n + j] *= ip; }
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      const double f = a[(size_t)r * n + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) {
+        a[(size_t)r * n + j] -= f * a[(size_t)c * n + j];
+        inv[(size_t)r * n + j] -= f * inv[(size_t)c * n + j];
+      }
+    }
+  }
+}
+
+// Numeric AMG set-up on the current (Dirichlet-imposed) tangent of precision T:
+// block-Jacobi inverses, Chebyshev bounds by power iteration, Galerkin
+// coarse operators, dense coarse inverse.  Rebuilt per load step by default
+// (the reference's reuse policy, Solver.jl:243-245).
+template <typename T>
+int amg_setup(pfem_ctx* ctx, int cheb_degree) {
+  if (!ctx->amg_struct) build_amg_structure(ctx);
+  int rc = amg_alloc<T>(ctx);
+  if (rc) return rc;
+  rc = krylov_alloc<T>(ctx);
+  if (rc) return rc;
+  Amg<T>& A = amg_of<T>(ctx);
+  KrylovWork<T>& w = kw_of<T>(ctx);
+  A.cheb_degree = cheb_degree;
+  A.lv[0].A.val = K_of<T>(ctx);
+  const int L = (int)A.lv.size();
+  for (int l = 0; l < L; ++l) {
+    AmgLevel<T>& v = A.lv[l];
+    blockdiag_invert<T>(v.A, v.dinv, ctx->st);
+    CKL();
+    // power iteration on D^-1 A
+    const long long n = (long long)v.A.nbrow * v.A.bs;
+    hash_fill_kernel<<<256, 256, 0, ctx->st>>>(n, std::is_same<T, float>::value ? (float*)v.d : nullptr,
+                                               std::is_same<T, double>::value ? (double*)v.d : nullptr);
+    for (int it = 0; it < 12; ++it) {
+      bsr_spmv<T>(v.A, v.d, v.t, ctx->st);
+      blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, v.t, v.r, T(1), nullptr, ctx->st);
+      dot<T>(n, v.r, v.r, w.sc + 8, w.part, ctx->st, true);
+      scale_by_inv_kernel<T><<<256, 256, 0, ctx->st>>>(n, w.sc + 8, v.r, v.d);
+    }
+    CKL();
+    T lm = 0;
+    CK(cudaMemcpyAsync(&lm, w.sc + 8, sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    v.lmax = (T)(1.1 * (double)lm);
+    // Galerkin coarse operator
+    T* cval;
+    long long cnnzb;
+    if (l + 1 < L) {
+      cval = A.lv[l + 1].A.val;
+      cnnzb = A.lv[l + 1].A.nnzb;
+    } else {
+      cval = A.lv[l].t;  // placeholder; coarsest handled below
+      cnnzb = 0;
+    }
+    if (l + 1 < L) {
+      CK(cudaMemsetAsync(cval, 0, (size_t)cnnzb * 36 * sizeof(T), ctx->st));
+      galerkin<T>(v.A, v.T, v.fine2coarse, cval, ctx->st);
+      CKL();
+    }
+  }
+  // coarsest operator: Galerkin product into a host-side dense matrix
+  {
+    const HostLevel& hc = ctx->hl[L];
+    const AmgLevel<T>& v = A.lv[L - 1];
+    const long long cnnzb = hc.rowptr[hc.nbrow];
+    T* cval = nullptr;
+    CK(cudaMalloc((void**)&cval, (size_t)std::max<long long>(cnnzb, 1) * 36 * sizeof(T)));
+    CK(cudaMemsetAsync(cval, 0, (size_t)cnnzb * 36 * sizeof(T), ctx->st));
+    galerkin<T>(v.A, v.T, v.fine2coarse, cval, ctx->st);
+    CKL();
+    std::vector<T> hv((size_t)cnnzb * 36);
+    CK(cudaMemcpyAsync(hv.data(), cval, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    cudaFree(cval);
+    const int n = A.coarse_n;
+    std::vector<double> dense((size_t)n * n, 0.0), inv;
+    for (int I = 0; I < hc.nbrow; ++I)
+      for (int k = hc.rowptr[I]; k < hc.rowptr[I + 1]; ++k) {
+        const int J = hc.col[k];
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 6; ++c) dense[(size_t)(I * 6 + r) * n + J * 6 + c] = (double)hv[(size_t)k * 36 + r * 6 + c];
+      }
+    // rigid modes absent from an aggregate leave zero rows: put 1 on their diagonal
+    for (int i = 0; i < n; ++i) {
+      bool zero = true;
+      for (int j = 0; j < n && zero; ++j) zero = dense[(size_t)i * n + j] == 0.0;
+      if (zero) dense[(size_t)i * n + i] = 1.0;
+    }
+    dense_inverse(n, dense, inv);
+    std::vector<T> invT(inv.begin(), inv.end());
+    CK(cudaMemcpyAsync(A.coarse_inv, invT.data(), invT.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  A.built = true;
+  return PFEM_OK;
+}
+
+// Chebyshev smoothing (block-Jacobi preconditioned) on level l:
+// x <- x + p(D^-1 A) D^-1 (b - A x), degree A.cheb_degree, interval
+// [lmax/30, lmax].  zero: x enters as 0.
+template <typename T>
+void cheb(pfem_ctx* ctx, AmgLevel<T>& v, int degree, const T* b, T* x, bool zero) {
+  const long long n = (long long)v.A.nbrow * v.A.bs;
+  const double lmx = (double)v.lmax, lmn = lmx / 30.0;
+  const double th = 0.5 * (lmx + lmn), de = 0.5 * (lmx - lmn);
+  const double sg = th / de;
+  double rho = 1.0 / sg;
+  if (zero) {
+    fill<T>(n, x, T(0), ctx->st);
+    blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, b, v.r, T(1.0 / th), v.d, ctx->st);
+  } else {
+    bsr_residual<T>(v.A, x, b, v.t, ctx->st);
+    blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, v.t, v.r, T(1.0 / th), v.d, ctx->st);
+  }
+  for (int k = 1; k <= degree; ++k) {
+    if (k < degree) {
+      bsr_cheb_step<T>(v.A, v.dinv, v.d, v.r, x, ctx->st);
+      const double rn = 1.0 / (2.0 * sg - rho);
+      axpby<T>(n, T(2.0 * rn / de), v.r, T(rn * rho), v.d, ctx->st);
+      rho = rn;
+    } else {
+      axpby<T>(n, T(1), v.d, T(1), x, ctx->st);
+    }
+  }
+}
+
+template <typename T>
+void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
+  Amg<T>& A = amg_of<T>(ctx);
+  const int L = (int)A.lv.size();
+  AmgLevel<T>& v = A.lv[l];
+  cheb<T>(ctx, v, A.cheb_degree, b, x, true);
+  bsr_residual<T>(v.A, x, b, v.t, ctx->st);
+  T* bn = (l + 1 < L) ? A.lv[l + 1].b : A.cb;
+  T* xn = (l + 1 < L) ? A.lv[l + 1].x : A.cx;
+  amg_restrict<T>(v.nagg, v.A.bs, v.agg_ptr, v.agg_mem, v.T, v.t, bn, ctx->st);
+  if (l + 1 < L) vcycle<T>(ctx, l + 1, bn, xn);
+  else dense_mv<T>(A.coarse_n, A.coarse_inv, bn, xn, ctx->st);
+  amg_prolong<T>(v.A.nbrow, v.A.bs, v.agg, v.T, xn, x, ctx->st);
+  cheb<T>(ctx, v, A.cheb_degree, b, x, false);
+}
+
+// Preconditioned CG / BiCGStab on level-0 operator with the AMG V-cycle.
+// b and the result x live in kw.b / kw.x.  Returns iterations (>=0) or <0.
+template <typename T>
+int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* conv) {
+  Amg<T>& A = amg_of<T>(ctx);
+  KrylovWork<T>& w = kw_of<T>(ctx);
+  const BsrMat<T>& K = A.lv[0].A;
+  const long long n = ctx->ndof;
+  cudaStream_t st = ctx->st;
+  *iters = 0;
+  *conv = false;
+  fill<T>(n, w.x, T(0), st);
+  CK(cudaMemcpyAsync(w.r, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  dot<T>(n, w.b, w.b, w.sc + 10, w.part, st, true);
+  T bn = 0;
+  CK(cudaMemcpyAsync(&bn, w.sc + 10, sizeof(T), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (!(bn > 0)) { *conv = true; return PFEM_OK; }
+  const double thr = rtol * (double)bn;
+  if (method == PFEM_KRYLOV_CG) {
+    vcycle<T>(ctx, 0, w.r, w.z);
+    dot<T>(n, w.r, w.z, w.sc + 0, w.part, st, false);
+    CK(cudaMemcpyAsync(w.p, w.z, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    for (int it = 1; it <= itmax; ++it) {
+      bsr_spmv<T>(K, w.p, w.q, st);
+      dot<T>(n, w.p, w.q, w.sc + 1, w.part, st, false);
+      cg_xr<T>(n, w.sc + 0, w.sc + 1, w.p, w.q, w.x, w.r, st);
+      dot<T>(n, w.r, w.r, w.sc + 3, w.part, st, true);
+      T rn = 0;
+      CK(cudaMemcpyAsync(&rn, w.sc + 3, sizeof(T), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      *iters = it;
+      if ((double)rn <= thr) { *conv = true; break; }
+      if (!std::isfinite((double)rn)) break;
+      vcycle<T>(ctx, 0, w.r, w.z);
+      dot<T>(n, w.r, w.z, w.sc + 2, w.part, st, false);
+      cg_p<T>(n, w.sc + 2, w.sc + 0, w.z, w.p, st);
+      scalar_copy<T>(w.sc + 0, w.sc + 2, st);
+    }
+  } else {
+    CK(cudaMemcpyAsync(w.rh, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    fill<T>(n, w.v, T(0), st);
+    fill<T>(n, w.p, T(0), st);
+    bicg_init_kernel<T><<<1, 1, 0, st>>>(w.sc);
+    for (int it = 1; it <= itmax; ++it) {
+      dot<T>(n, w.rh, w.r, w.sc + 0, w.part, st, false);
+      bicg_p<T>(n, w.sc, w.r, w.v, w.p, st);
+      vcycle<T>(ctx, 0, w.p, w.ph);
+      bsr_spmv<T>(K, w.ph, w.v, st);
+      dot<T>(n, w.rh, w.v, w.sc + 4, w.part, st, false);
+      bicg_s<T>(n, w.sc, w.r, w.v, w.s, st);
+      vcycle<T>(ctx, 0, w.s, w.sh);
+      bsr_spmv<T>(K, w.sh, w.t, st);
+      dot<T>(n, w.t, w.s, w.sc + 5, w.part, st, false);
+      dot<T>(n, w.t, w.t, w.sc + 6, w.part, st, false);
+      bicg_xr<T>(n, w.sc, w.ph, w.sh, w.s, w.t, w.x, w.r, st);
+      bicg_finish_kernel<T><<<1, 1, 0, st>>>(w.sc);
+      dot<T>(n, w.r, w.r, w.sc + 3, w.part, st, true);
+      T rn = 0;
+      CK(cudaMemcpyAsync(&rn, w.sc + 3, sizeof(T), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      *iters = it;
+      if ((double)rn <= thr) { *conv = true; break; }
+      if (!std::isfinite((double)rn)) break;
+    }
+  }
+  CKL();
+  return PFEM_OK;
+}
+
+// One full assembly: zero K (precision prec) and R, run the element kernel over
+// every color; commit runs the state update over all elements in one launch.
+int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
+  cudaStream_t st = ctx->st;
+  const bool fbar = ctx->kind == PFEM_HEX8_FINITE_FBAR;
+  CK(cudaMemsetAsync(ctx->dStatus, 0, sizeof(DevStatus), st));
+  if (commit) {
+    ElemArgs<double> a{};
+    a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
+    a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+    a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
+    a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
+    launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, true, fbar, st);
+    CKL();
+    return PFEM_OK;
+  }
+  CK(cudaMemsetAsync(ctx->dR, 0, ctx->ndof * sizeof(double), st));
+  const int nc = (int)ctx->color_ptr.size() - 1;
+  if (prec == PFEM_FP64) {
+    CK(cudaMemsetAsync(ctx->dK64, 0, (size_t)ctx->nnzb * 9 * sizeof(double), st));
+    ElemArgs<double> a{};
+    a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
+    a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+    a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
+    a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
+    for (int c = 0; c < nc; ++c)
+      launch_element_color<double>(a, ctx->dColorList + ctx->color_ptr[c], ctx->color_ptr[c + 1] - ctx->color_ptr[c],
+                                   false, fbar, st);
+  } else {
+    CK(cudaMemsetAsync(ctx->dK32, 0, (size_t)ctx->nnzb * 9 * sizeof(float), st));
+    ElemArgs<float> a{};
+    a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
+    a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+    a.R = ctx->dR; a.Kval = ctx->dK32; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
+    a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
+    for (int c = 0; c < nc; ++c)
+      launch_element_color<float>(a, ctx->dColorList + ctx->color_ptr[c], ctx->color_ptr[c + 1] - ctx->color_ptr[c],
+                                  false, fbar, st);
+  }
+  CKL();
+  return PFEM_OK;
+}
+
+int ensure_tangent(pfem_ctx* ctx, int prec) {
+  if (prec == PFEM_FP64 && !ctx->dK64) CK(dalloc(ctx, &ctx->dK64, (size_t)ctx->nnzb * 9));
+  if (prec == PFEM_MIXED && !ctx->dK32) CK(dalloc(ctx, &ctx->dK32, (size_t)ctx->nnzb * 9));
+  return PFEM_OK;
+}
+
+int check_status(pfem_ctx* ctx) {
+  DevStatus s;
+  CK(cudaMemcpyAsync(&s, ctx->dStatus, sizeof(s), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (s.code) {
+    char buf[256];
+    snprintf(buf, sizeof(buf),
+             "ElementInversionError: element %lld, Gauss point %d is inverted (det F = J = %.6g <= 0)",
+             s.e, s.g, s.J);
+    return fail(ctx, PFEM_ERR_INVERTED_ELEMENT, buf);
+  }
+  return PFEM_OK;
+}
+
+// Assemble + impose Dirichlet at lambda; returns ||R|| of the imposed system.
+int residual_system(pfem_ctx* ctx, int prec, double lam, double* rnorm, double* t_asm) {
+  int rc = ensure_tangent(ctx, prec);
+  if (rc) return rc;
+  CK(cudaEventRecord(ctx->e0, ctx->st));
+  rc = assemble_dev(ctx, prec, false);
+  if (rc) return rc;
+  CK(cudaEventRecord(ctx->e1, ctx->st));
+  if (prec == PFEM_FP64) impose_dirichlet<double>(ctx->bc, ctx->ndof, lam, ctx->dU, ctx->dK64, ctx->dR, ctx->dDg, ctx->st);
+  else impose_dirichlet<float>(ctx->bc, ctx->ndof, lam, ctx->dU, ctx->dK32, ctx->dR, ctx->dDg, ctx->st);
+  CKL();
+  dot<double>(ctx->ndof, ctx->dR, ctx->dR, ctx->dScal, ctx->dPart, ctx->st, true);
+  CKL();
+  CK(cudaMemcpyAsync(rnorm, ctx->dScal, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  rc = check_status(ctx);  // synchronizes
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->e0, ctx->e1);
+  if (t_asm) *t_asm += ms;
+  ctx->tangent_prec = prec;
+  return rc;
+}
+
+// Solve K dU = -R (device R) with precision prec; the correction stays in
+// the precision-T Krylov vector kw.x.
+int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool rebuild, int* kits,
+                      double* t_amg, double* t_kry) {
+  const int prec = o->precision;
+  int rc;
+  auto t0 = std::chrono::steady_clock::now();
+  if (prec == PFEM_FP64) {
+    if (rebuild || !ctx->amg64.built) {
+      rc = amg_setup<double>(ctx, o->cheb_degree);
+      if (rc) return rc;
+    } else {
+      ctx->amg64.lv[0].A.val = ctx->dK64;
+    }
+  } else {
+    if (rebuild || !ctx->amg32.built) {
+      rc = amg_setup<float>(ctx, o->cheb_degree);
+      if (rc) return rc;
+    } else {
+      ctx->amg32.lv[0].A.val = ctx->dK32;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  auto t1 = std::chrono::steady_clock::now();
+  *t_amg += std::chrono::duration<double, std::milli>(t1 - t0).count();
+  bool conv = false;
+  if (prec == PFEM_FP64) {
+    convert<double, double>(ctx->ndof, ctx->dR, ctx->kw64.b, -1.0, ctx->st);
+    rc = krylov<double>(ctx, o->krylov, rtol, o->krylov_itmax, kits, &conv);
+  } else {
+    convert<double, float>(ctx->ndof, ctx->dR, ctx->kw32.b, -1.0, ctx->st);
+    rc = krylov<float>(ctx, o->krylov, rtol, o->krylov_itmax, kits, &conv);
+  }
+  if (rc) return rc;
+  CKL();
+  CK(cudaStreamSynchronize(ctx->st));
+  auto t2 = std::chrono::steady_clock::now();
+  *t_kry += std::chrono::duration<double, std::milli>(t2 - t1).count();
+  (void)conv;  // an inexact inner solve is still a descent step; Newton judges it
+  return PFEM_OK;
+}
+
+template <typename T>
+__global__ void step_kernel(long long n, double a, const T* __restrict__ x, const double* __restrict__ u0,
+                            double* __restrict__ u) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    u[i] = u0[i] + a * (double)x[i];
+}
+
+double forcing_term(const pfem_solve_opts* o, int it, double rk, double rkm1, double eta_prev) {
+  // _forcing_term, Solver.jl:159-171
+  if (it == 1 || rkm1 <= 0) return o->eta_max;
+  double eta = o->ew_gamma * std::pow(rk / rkm1, o->ew_alpha);
+  const double safe = o->ew_gamma * std::pow(eta_prev, o->ew_alpha);
+  if (safe > 0.1) eta = std::max(eta, safe);
+  return std::min(std::max(eta, o->eta_min), o->eta_max);
+}
+
+struct StepTimes {
+  double asm_ms = 0, amg_ms = 0, kry_ms = 0, pred_ms = 0;
+  int kits = 0;
+};
+
+// newton! (Solver.jl:317-389) at lambda from the current device U.  With
+// o->line_search the step length is halved (at most 8 times) until the
+// imposed FP64 residual norm drops; the full step is tried first and its
+// assembly becomes the next iterate, so line search costs extra assemblies
+// only when it backtracks.
+int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, double* hist,
+               int* khist, bool* converged, StepTimes* tm) {
+  *converged = false;
+  const double fext_norm = std::fabs(lam) * ctx->fn_norm;
+  double ref = 1.0, rkm1 = 0.0, eta_prev = o->eta_max;
+  bool first = true;
+  double rn = 0;
+  int rc = residual_system(ctx, o->precision, lam, &rn, &tm->asm_ms);
+  if (rc) return rc;
+  int it;
+  for (it = 1; it <= o->maxiter; ++it) {
+    if (hist) hist[it - 1] = rn;
+    if (it == 1) ref = std::max(std::max(rn, fext_norm), 1.0);
+    if (o->verbose) fprintf(stderr, "    iter %d  |R| = %.6e\n", it, rn);
+    if (!std::isfinite(rn)) return fail(ctx, PFEM_ERR_NOT_CONVERGED, "non-finite residual");
+    if (rn <= o->tol * ref) {
+      *converged = true;
+      break;
+    }
+    if (it == o->maxiter) break;
+    double eta = o->lin_rtol > 0 ? o->lin_rtol : forcing_term(o, it, rn, rkm1, eta_prev);
+    const bool rebuild = first || o->amg_rebuild;
+    first = false;
+    int kits = 0;
+    rc = newton_correction(ctx, o, eta, rebuild, &kits, &tm->amg_ms, &tm->kry_ms);
+    if (rc) return rc;
+    if (khist) khist[it - 1] = kits;
+    tm->kits += kits;
+    rkm1 = rn;
+    eta_prev = eta;
+    CK(cudaMemcpyAsync(ctx->dUtmp, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+    double a = 1.0, rt = 0.0;
+    for (int bt = 0;; ++bt) {
+      if (o->precision == PFEM_FP64)
+        step_kernel<double><<<1024, 256, 0, ctx->st>>>(ctx->ndof, a, ctx->kw64.x, ctx->dUtmp, ctx->dU);
+      else
+        step_kernel<float><<<1024, 256, 0, ctx->st>>>(ctx->ndof, a, ctx->kw32.x, ctx->dUtmp, ctx->dU);
+      CKL();
+      rc = residual_system(ctx, o->precision, lam, &rt, &tm->asm_ms);
+      if (!o->line_search) {
+        if (rc) return rc;
+        break;
+      }
+      const bool inverted = rc == PFEM_ERR_INVERTED_ELEMENT;
+      if (rc && !inverted) return rc;
+      if (!inverted && std::isfinite(rt) && (rt < (1.0 - 1e-4 * a) * rn || bt >= 8)) break;
+      if (bt >= 8) return rc ? rc : fail(ctx, PFEM_ERR_NOT_CONVERGED, "line search failed");
+      a *= 0.5;
+    }
+    rn = rt;
+  }
+  *iters = std::min(it, o->maxiter);
+  return PFEM_OK;
+}
+
+int commit_dev(pfem_ctx* ctx) {
+  int rc = assemble_dev(ctx, PFEM_FP64, true);
+  if (rc) return rc;
+  return check_status(ctx);
+}
+
+__global__ void extrap_kernel(long long n, double f, const double* __restrict__ u1,
+                              const double* __restrict__ u2, double* __restrict__ u) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    u[i] = u1[i] + f * (u1[i] - u2[i]);
+}
+
+__global__ void init_state_kernel(long long ngp, double* cpi, double* alpha, double* epsp, double* tau) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ngp; i += (long long)gridDim.x * blockDim.x) {
+    for (int c = 0; c < 6; ++c) {
+      cpi[c * ngp + i] = c < 3 ? 1.0 : 0.0;
+      epsp[c * ngp + i] = 0.0;
+      tau[c * ngp + i] = 0.0;
+    }
+    alpha[i] = 0.0;
+  }
+}
+
+}  // namespace
+
+// =====================================================================  C ABI
+extern "C" {
+
+void pfem_default_opts(pfem_solve_opts* o) {
+  o->nsteps = 10;
+  o->maxiter = 25;
+  o->tol = 1e-8;
+  o->precision = PFEM_FP64;
+  o->krylov = PFEM_KRYLOV_CG;
+  o->lin_rtol = -1.0;
+  o->eta_min = 1e-8;
+  o->eta_max = 0.1;
+  o->ew_gamma = 0.9;
+  o->ew_alpha = 1.5;
+  o->krylov_itmax = 200;
+  o->predictor = PFEM_PRED_PREVIOUS;
+  o->amg_rebuild = 0;
+  o->cheb_degree = 2;
+  o->verbose = 0;
+  o->line_search = 0;
+}
+
+const char* pfem_last_error(const pfem_ctx* ctx) {
+  if (!ctx) return g_cuda_err.c_str();
+  return ctx->err.c_str();
+}
+
+int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* elements, int64_t ne,
+                int32_t kind, const pfem_material* m, const double* sigy0_e, int32_t device) {
+  if (!out || !nodes || !elements || !m || nn <= 0 || ne <= 0) return PFEM_ERR_BAD_ARG;
+  *out = nullptr;
+  // J2Material guards, Materials.jl:90-103
+  if (!(m->E > 0) || !(m->nu > -1 && m->nu < 0.5) || !(m->sigy0 > 0) || !(m->Hiso >= 0) || !(m->Hkin >= 0)) {
+    g_cuda_err = "invalid material parameters (E>0, -1<nu<0.5, sigy0>0, Hiso>=0, Hkin>=0)";
+    return PFEM_ERR_BAD_ARG;
+  }
+  if (m->Hkin != 0.0) {
+    g_cuda_err = "this path implements linear isotropic hardening only (Hkin must be 0)";
+    return PFEM_ERR_BAD_ARG;
+  }
+  if (kind != PFEM_HEX8_FINITE && kind != PFEM_HEX8_FINITE_FBAR) {
+    g_cuda_err = "kind must be PFEM_HEX8_FINITE or PFEM_HEX8_FINITE_FBAR";
+    return PFEM_ERR_BAD_ARG;
+  }
+  for (int64_t i = 0; i < 8 * ne; ++i)
+    if (elements[i] < 1 || elements[i] > nn) {
+      g_cuda_err = "element connectivity out of range (1-based node ids expected)";
+      return PFEM_ERR_BAD_ARG;
+    }
+  if (sigy0_e)
+    for (int64_t e = 0; e < ne; ++e)
+      if (!(sigy0_e[e] > 0)) {
+        g_cuda_err = "per-element sigy0 must be positive";
+        return PFEM_ERR_BAD_ARG;
+      }
+  pfem_ctx* ctx = new pfem_ctx();
+  ctx->device = device;
+  ctx->nn = nn; ctx->ne = ne; ctx->ngp = 8 * ne; ctx->ndof = 3 * nn;
+  ctx->kind = kind;
+  ctx->mat.E = m->E; ctx->mat.nu = m->nu; ctx->mat.sigy0 = m->sigy0; ctx->mat.Hiso = m->Hiso; ctx->mat.Hkin = m->Hkin;
+  ctx->mat.G = m->E / (2.0 * (1.0 + m->nu));
+  ctx->mat.K = m->E / (3.0 * (1.0 - 2.0 * m->nu));
+  ctx->mat.lam = m->E * m->nu / ((1.0 + m->nu) * (1.0 - 2.0 * m->nu));
+  auto bail = [&](int rc) {
+    if (ctx->err.empty()) ctx->err = g_cuda_err;
+    g_cuda_err = ctx->err;
+    pfem_destroy(ctx);
+    return rc;
+  };
+  if (device >= 0) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { pfem_set_cuda_error(e, "cudaSetDevice", __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
+    e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { pfem_set_cuda_error(e, "cudaStreamCreate", __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
+    cudaEventCreate(&ctx->e0);
+    cudaEventCreate(&ctx->e1);
+  }
+  if ((long long)ctx->ndof >= (1ll << 31)) return bail(fail(ctx, PFEM_ERR_BAD_ARG, "mesh too large for 32-bit dof indices"));
+  // ---- host topology ----
+  ctx->X.assign(nodes, nodes + 3 * nn);
+  ctx->elem.resize(8 * ne);
+  for (int64_t i = 0; i < 8 * ne; ++i) ctx->elem[i] = (int)(elements[i] - 1);
+  // node adjacency via node->element incidence
+  std::vector<int> nptr(nn + 1, 0);
+  for (int64_t e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) nptr[ctx->elem[e * 8 + a] + 1]++;
+  for (int64_t n = 0; n < nn; ++n) nptr[n + 1] += nptr[n];
+  std::vector<int> nel(nptr[nn]);
+  {
+    std::vector<int> f(nptr.begin(), nptr.end() - 1);
+    for (int64_t e = 0; e < ne; ++e)
+      for (int a = 0; a < 8; ++a) nel[f[ctx->elem[e * 8 + a]]++] = (int)e;
+  }
+  std::vector<int> deg(nn);
+  std::vector<std::vector<int>> adj(nn);
+  par_for(nn, [&](long long n) {
+    std::vector<int>& v = adj[n];
+    v.reserve(64);
+    for (int k = nptr[n]; k < nptr[n + 1]; ++k)
+      for (int b = 0; b < 8; ++b) v.push_back(ctx->elem[(long long)nel[k] * 8 + b]);
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    deg[n] = (int)v.size();
+  });
+  ctx->browptr.assign(nn + 1, 0);
+  for (int64_t n = 0; n < nn; ++n) ctx->browptr[n + 1] = ctx->browptr[n] + deg[n];
+  ctx->nnzb = ctx->browptr[nn];
+  if (ctx->nnzb * 9 >= (1ll << 31)) return bail(fail(ctx, PFEM_ERR_BAD_ARG, "pattern too large for 32-bit indices"));
+  ctx->bcol.resize(ctx->nnzb);
+  par_for(nn, [&](long long n) { std::copy(adj[n].begin(), adj[n].end(), ctx->bcol.begin() + ctx->browptr[n]); });
+  std::vector<uint8_t> rank((size_t)ne * 64);
+  par_for(ne, [&](long long e) {
+    for (int a = 0; a < 8; ++a) {
+      const auto& v = adj[ctx->elem[e * 8 + a]];
+      for (int b = 0; b < 8; ++b)
+        rank[(size_t)e * 64 + a * 8 + b] =
+            (uint8_t)(std::lower_bound(v.begin(), v.end(), ctx->elem[e * 8 + b]) - v.begin());
+    }
+  });
+  adj.clear();
+  adj.shrink_to_fit();
+  // colors: the reference's rule is reported; the device uses it when it
+  // yields independent sets (> 1 color), else a greedy coloring.
+  ctx->ncolors_ref = reference_colors(ctx->X, nn, ne, ctx->color_ref);
+  std::vector<int> col;
+  int nc;
+  if (ctx->ncolors_ref > 1) {
+    col.assign(ctx->color_ref.begin(), ctx->color_ref.end());
+    nc = ctx->ncolors_ref;
+  } else {
+    nc = greedy_colors(ctx->elem, nn, ne, col);
+  }
+  ctx->color_ptr.assign(nc + 1, 0);
+  for (int64_t e = 0; e < ne; ++e) ctx->color_ptr[col[e] + 1]++;
+  for (int c = 0; c < nc; ++c) ctx->color_ptr[c + 1] += ctx->color_ptr[c];
+  std::vector<int> clist(ne), all(ne);
+  {
+    std::vector<int> f(ctx->color_ptr.begin(), ctx->color_ptr.end() - 1);
+    for (int64_t e = 0; e < ne; ++e) clist[f[col[e]]++] = (int)e;
+  }
+  std::iota(all.begin(), all.end(), 0);
+  if (device < 0) {  // topology-only context: pattern / colors, no device work
+    *out = ctx;
+    return PFEM_OK;
+  }
+  // ---- device upload ----
+  cudaError_t ce;
+#define UP(ptr, vec) if ((ce = upload(ctx, &ptr, vec)) != cudaSuccess) { pfem_set_cuda_error(ce, #ptr, __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
+#define AL(ptr, n) if ((ce = dalloc(ctx, &ptr, n)) != cudaSuccess) { pfem_set_cuda_error(ce, #ptr, __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
+  UP(ctx->dX, ctx->X);
+  UP(ctx->dElem, ctx->elem);
+  UP(ctx->dRank, rank);
+  UP(ctx->dBrowptr, ctx->browptr);
+  UP(ctx->dBcol, ctx->bcol);
+  UP(ctx->dColorList, clist);
+  UP(ctx->dAllElems, all);
+  if (sigy0_e) {
+    std::vector<double> s(sigy0_e, sigy0_e + ne);
+    UP(ctx->dSigy, s);
+  }
+  AL(ctx->dCpi, 6 * ctx->ngp);
+  AL(ctx->dAlpha, ctx->ngp);
+  AL(ctx->dEpsp, 6 * ctx->ngp);
+  AL(ctx->dTau, 6 * ctx->ngp);
+  AL(ctx->dFlags, ctx->ngp);
+  AL(ctx->dU, ctx->ndof);
+  AL(ctx->dR, ctx->ndof);
+  AL(ctx->dDg, ctx->ndof);
+  AL(ctx->dUprev, ctx->ndof);
+  AL(ctx->dUprev2, ctx->ndof);
+  AL(ctx->dUtmp, ctx->ndof);
+  AL(ctx->dScal, 16);
+  AL(ctx->dPart, 2048);
+  AL(ctx->dStatus, 1);
+#undef UP
+#undef AL
+  int rc = pfem_reset(ctx);
+  if (rc) return bail(rc);
+  *out = ctx;
+  return PFEM_OK;
+}
+
+void pfem_destroy(pfem_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->device < 0) {
+    delete ctx;
+    return;
+  }
+  cudaSetDevice(ctx->device);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  for (void* p : ctx->allocs) cudaFree(p);
+  pfem::mlp_free(ctx->mlp);
+  if (ctx->e0) cudaEventDestroy(ctx->e0);
+  if (ctx->e1) cudaEventDestroy(ctx->e1);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+}
+
+int pfem_inversion_info(const pfem_ctx* ctx, int64_t* e, int32_t* g, double* J) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return PFEM_ERR_STATE;
+  DevStatus s;
+  if (cudaMemcpy(&s, ctx->dStatus, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (e) *e = s.code ? s.e : 0;
+  if (g) *g = s.code ? s.g : 0;
+  if (J) *J = s.code ? s.J : 0.0;
+  return PFEM_OK;
+}
+
+int pfem_pattern(const pfem_ctx* ctx, int64_t* nnz, int64_t* colptr, int64_t* rowval) {
+  if (!ctx || !nnz) return PFEM_ERR_BAD_ARG;
+  *nnz = ctx->nnzb * 9;
+  if (!colptr && !rowval) return PFEM_OK;
+  // Column j = 3n+c holds rows 3m+1..3m+3 for every neighbour m of n
+  // (ascending): the count-then-fill layout of Assembly.jl:119-146.
+  if (colptr) {
+    colptr[0] = 1;
+    for (long long n = 0; n < ctx->nn; ++n) {
+      const int64_t d = 3 * (int64_t)(ctx->browptr[n + 1] - ctx->browptr[n]);
+      for (int c = 0; c < 3; ++c) colptr[3 * n + c + 1] = colptr[3 * n + c] + d;
+    }
+  }
+  if (rowval) {
+    int64_t p = 0;
+    for (long long n = 0; n < ctx->nn; ++n)
+      for (int c = 0; c < 3; ++c)
+        for (int k = ctx->browptr[n]; k < ctx->browptr[n + 1]; ++k) {
+          const int64_t r0 = 3 * (int64_t)ctx->bcol[k];
+          rowval[p++] = r0 + 1;
+          rowval[p++] = r0 + 2;
+          rowval[p++] = r0 + 3;
+        }
+  }
+  return PFEM_OK;
+}
+
+int pfem_colors(const pfem_ctx* ctx, int32_t* ncolors, int64_t* color_of_element) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ncolors) *ncolors = ctx->ncolors_ref;
+  if (color_of_element) std::copy(ctx->color_ref.begin(), ctx->color_ref.end(), color_of_element);
+  return PFEM_OK;
+}
+
+int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals, const uint8_t* dir_ramp,
+                 int64_t ndir, const int64_t* neu_dofs, const double* neu_vals, int64_t nneu) {
+  if (!ctx || ndir < 0 || nneu < 0) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  const long long ndof = ctx->ndof;
+  // _freeze_bcs: last assignment wins (Solver.jl:192-218)
+  std::vector<int> last(ndof, -1);
+  for (int64_t i = 0; i < ndir; ++i) {
+    const int64_t d = dir_dofs[i] - 1;
+    if (d < 0 || d >= ndof) return fail(ctx, PFEM_ERR_BAD_ARG, "Dirichlet dof out of range");
+    last[d] = (int)i;
+  }
+  std::vector<int> dofs;
+  std::vector<double> vals;
+  std::vector<uint8_t> ramp;
+  std::vector<uint8_t> isbc(ndof, 0);
+  for (long long d = 0; d < ndof; ++d)
+    if (last[d] >= 0) {
+      dofs.push_back((int)d);
+      vals.push_back(dir_vals[last[d]]);
+      ramp.push_back(dir_ramp ? dir_ramp[last[d]] : 1);
+      isbc[d] = 1;
+    }
+  std::vector<double> fn(ndof, 0.0);
+  for (int64_t i = 0; i < nneu; ++i) {
+    const int64_t d = neu_dofs[i] - 1;
+    if (d < 0 || d >= ndof) return fail(ctx, PFEM_ERR_BAD_ARG, "Neumann dof out of range");
+    fn[d] += neu_vals[i];
+  }
+  double s = 0;
+  for (double v : fn) s += v * v;
+  ctx->fn_norm = std::sqrt(s);
+  // entries touched by the imposition
+  auto blk = [&](int n, int m) -> long long {
+    const int* b0 = ctx->bcol.data() + ctx->browptr[n];
+    const int* b1 = ctx->bcol.data() + ctx->browptr[n + 1];
+    return ctx->browptr[n] + (long long)(std::lower_bound(b0, b1, m) - b0);
+  };
+  std::vector<std::pair<long long, uint8_t>> zl;
+  std::vector<std::tuple<int, int, long long>> rl;  // (row, col, pos)
+  for (int d : dofs) {
+    const int n = d / 3, c = d % 3;
+    for (int k = ctx->browptr[n]; k < ctx->browptr[n + 1]; ++k) {
+      const int m = ctx->bcol[k];
+      for (int j = 0; j < 3; ++j) zl.push_back({(long long)k * 9 + c * 3 + j, (uint8_t)(3 * m + j == d)});
+      // column d: block (m, n), entry (i, c)
+      const long long bk = blk(m, n);
+      for (int i = 0; i < 3; ++i) {
+        const int r = 3 * m + i;
+        const long long pos = bk * 9 + i * 3 + c;
+        zl.push_back({pos, (uint8_t)(r == d)});
+        if (!isbc[r]) rl.emplace_back(r, d, pos);
+      }
+    }
+  }
+  std::sort(zl.begin(), zl.end());
+  zl.erase(std::unique(zl.begin(), zl.end(), [](auto& a, auto& b) { return a.first == b.first; }), zl.end());
+  std::sort(rl.begin(), rl.end());
+  std::vector<int> rows, rptr(1, 0), rcol;
+  std::vector<long long> rpos, zpos;
+  std::vector<uint8_t> zone;
+  for (size_t i = 0; i < rl.size(); ++i) {
+    const int r = std::get<0>(rl[i]);
+    if (rows.empty() || rows.back() != r) {
+      if (!rows.empty()) rptr.push_back((int)rpos.size());
+      rows.push_back(r);
+    }
+    rpos.push_back(std::get<2>(rl[i]));
+    rcol.push_back(std::get<1>(rl[i]));
+  }
+  rptr.push_back((int)rpos.size());
+  if (rows.empty()) rptr.assign(1, 0);
+  for (auto& z : zl) { zpos.push_back(z.first); zone.push_back(z.second); }
+  BcDev& b = ctx->bc;
+  b = BcDev();
+  b.nbc = (int)dofs.size();
+  b.nrows = (int)rows.size();
+  b.nzero = (long long)zpos.size();
+  CK(upload(ctx, &b.dofs, dofs));
+  CK(upload(ctx, &b.vals, vals));
+  CK(upload(ctx, &b.ramp, ramp));
+  CK(upload(ctx, &b.fn, fn));
+  CK(upload(ctx, &b.rows, rows));
+  CK(upload(ctx, &b.rptr, rptr));
+  CK(upload(ctx, &b.rpos, rpos));
+  CK(upload(ctx, &b.rcol, rcol));
+  CK(upload(ctx, &b.zpos, zpos));
+  CK(upload(ctx, &b.zone, zone));
+  ctx->bcs_set = true;
+  return PFEM_OK;
+}
+
+int pfem_reset(pfem_ctx* ctx) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  init_state_kernel<<<1024, 256, 0, ctx->st>>>(ctx->ngp, ctx->dCpi, ctx->dAlpha, ctx->dEpsp, ctx->dTau);
+  CKL();
+  CK(cudaMemsetAsync(ctx->dFlags, 0, ctx->ngp, ctx->st));
+  CK(cudaMemsetAsync(ctx->dU, 0, ctx->ndof * sizeof(double), ctx->st));
+  CK(cudaMemsetAsync(ctx->dUprev, 0, ctx->ndof * sizeof(double), ctx->st));
+  CK(cudaMemsetAsync(ctx->dUprev2, 0, ctx->ndof * sizeof(double), ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->steps_taken = 0;
+  ctx->lam_prev = ctx->lam_prev2 = 0.0;
+  return PFEM_OK;
+}
+
+int pfem_set_state(pfem_ctx* ctx, const double* cpi, const double* alpha, const double* epsp) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  const long long ngp = ctx->ngp;
+  auto put = [&](const double* h, double* d) -> int {
+    std::vector<double> t(6 * ngp);
+    for (long long g = 0; g < ngp; ++g)
+      for (int k = 0; k < 6; ++k) t[k * ngp + g] = h[g * 6 + k];
+    CK(cudaMemcpy(d, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return PFEM_OK;
+  };
+  int rc;
+  if (cpi && (rc = put(cpi, ctx->dCpi))) return rc;
+  if (epsp && (rc = put(epsp, ctx->dEpsp))) return rc;
+  if (alpha) CK(cudaMemcpy(ctx->dAlpha, alpha, ngp * sizeof(double), cudaMemcpyHostToDevice));
+  return PFEM_OK;
+}
+
+int pfem_set_displacement(pfem_ctx* ctx, const double* U) {
+  if (!ctx || !U) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpyAsync(ctx->dU, U, ctx->ndof * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return PFEM_OK;
+}
+
+int pfem_assemble(pfem_ctx* ctx, const double* U, int32_t commit, int32_t precision, double* R, double* Kvals,
+                  double* tau, uint8_t* flags) {
+  if (!ctx || !U) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc = pfem_set_displacement(ctx, U);
+  if (rc) return rc;
+  const int prec = precision == PFEM_MIXED ? PFEM_MIXED : PFEM_FP64;
+  if (commit) {
+    rc = commit_dev(ctx);
+    if (rc) return rc;
+  } else {
+    rc = ensure_tangent(ctx, prec);
+    if (rc) return rc;
+    rc = assemble_dev(ctx, prec, false);
+    if (rc) return rc;
+    rc = check_status(ctx);
+    if (rc) return rc;
+    ctx->tangent_prec = -1;  // not imposed
+  }
+  if (R && !commit) CK(cudaMemcpy(R, ctx->dR, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Kvals && !commit) {
+    const size_t nv = (size_t)ctx->nnzb * 9;
+    std::vector<double> kv(nv);
+    if (prec == PFEM_FP64) {
+      CK(cudaMemcpy(kv.data(), ctx->dK64, nv * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> kf(nv);
+      CK(cudaMemcpy(kf.data(), ctx->dK32, nv * sizeof(float), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < nv; ++i) kv[i] = kf[i];
+    }
+    // block (n, m) entry (i, k) -> CSR row 3n+i, position 3*t + k in that row
+    int64_t p = 0;
+    for (long long n = 0; n < ctx->nn; ++n)
+      for (int i = 0; i < 3; ++i)
+        for (int k = ctx->browptr[n]; k < ctx->browptr[n + 1]; ++k)
+          for (int c = 0; c < 3; ++c) Kvals[p++] = kv[(size_t)k * 9 + i * 3 + c];
+  }
+  return pfem_get_state(ctx, nullptr, tau, nullptr, nullptr, nullptr, flags);
+}
+
+static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepTimes* tm) {
+  // predictor for this load step (previous U is the reference's choice)
+  const long long n = ctx->ndof;
+  auto t0 = std::chrono::steady_clock::now();
+  if (o->predictor != PFEM_PRED_PREVIOUS && ctx->steps_taken >= 1) {
+    const double dl = ctx->lam_prev - ctx->lam_prev2;
+    const double f = dl > 0 ? (lam - ctx->lam_prev) / dl : 0.0;
+    extrap_kernel<<<1024, 256, 0, ctx->st>>>(n, f, ctx->dUprev, ctx->dUprev2, ctx->dU);
+    bc_apply(ctx->bc, lam, ctx->dU, ctx->st);
+    CKL();
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  tm->pred_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return PFEM_OK;
+}
+
+static int step_end(pfem_ctx* ctx, double lam) {
+  CK(cudaMemcpyAsync(ctx->dUprev2, ctx->dUprev, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->dUprev, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+  ctx->lam_prev2 = ctx->lam_prev;
+  ctx->lam_prev = lam;
+  ctx->steps_taken++;
+  return PFEM_OK;
+}
+
+int pfem_newton(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, int32_t* iters, double* res_hist,
+                int32_t* krylov_hist) {
+  if (!ctx || !o) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  if (!ctx->bcs_set) return fail(ctx, PFEM_ERR_STATE, "pfem_set_bcs must be called first");
+  cudaSetDevice(ctx->device);
+  StepTimes tm;
+  int rc = step_begin(ctx, lambda, o, &tm);
+  if (rc) return rc;
+  std::vector<int> kh(o->maxiter, 0);
+  bool conv = false;
+  int it = 0;
+  rc = newton_dev(ctx, lambda, o, &it, res_hist, kh.data(), &conv, &tm);
+  if (iters) *iters = it;
+  if (krylov_hist) std::copy(kh.begin(), kh.end(), krylov_hist);
+  if (rc) return rc;
+  if (!conv) return fail(ctx, PFEM_ERR_NOT_CONVERGED, "load step did not converge");
+  rc = commit_dev(ctx);
+  if (rc) return rc;
+  return step_end(ctx, lambda);
+}
+
+int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res, int32_t* iters_per_step,
+               double* residuals, int32_t* krylov_per_iter) {
+  if (!ctx || !o || o->nsteps <= 0 || o->maxiter <= 0) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  if (!ctx->bcs_set) return fail(ctx, PFEM_ERR_STATE, "pfem_set_bcs must be called first");
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  pfem_solve_result r;
+  std::memset(&r, 0, sizeof(r));
+  r.converged = 1;
+  int rc = pfem_reset(ctx);
+  if (rc) return rc;
+  StepTimes tm;
+  for (int n = 1; n <= o->nsteps; ++n) {
+    const double lam = (double)n / o->nsteps;
+    if (o->verbose) fprintf(stderr, "Load step %d/%d  (lambda=%g)\n", n, o->nsteps, lam);
+    rc = step_begin(ctx, lam, o, &tm);
+    if (rc) return rc;
+    bool conv = false;
+    int it = 0;
+    rc = newton_dev(ctx, lam, o, &it, residuals ? residuals + (size_t)(n - 1) * o->maxiter : nullptr,
+                    krylov_per_iter ? krylov_per_iter + (size_t)(n - 1) * o->maxiter : nullptr, &conv, &tm);
+    if (rc) return rc;
+    if (iters_per_step) iters_per_step[n - 1] = it;
+    r.newton_iters_total += it;
+    if (!conv) {
+      r.converged = 0;
+      break;
+    }
+    rc = commit_dev(ctx);
+    if (rc) return rc;
+    rc = step_end(ctx, lam);
+    if (rc) return rc;
+    r.steps_done = n;
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  r.krylov_iters_total = tm.kits;
+  r.time_assembly_ms = tm.asm_ms;
+  r.time_amg_setup_ms = tm.amg_ms;
+  r.time_krylov_ms = tm.kry_ms;
+  r.time_predictor_ms = tm.pred_ms;
+  r.predictor_learned_used = ctx->mlp.used_count;
+  r.time_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (res) *res = r;
+  return r.converged ? PFEM_OK : fail(ctx, PFEM_ERR_NOT_CONVERGED, "a load step did not converge");
+}
+
+int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, int32_t rebuild_pc,
+                      const pfem_solve_opts* o, int32_t* niter) {
+  if (!ctx || !b || !x || !o) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  if (ctx->tangent_prec < 0) return fail(ctx, PFEM_ERR_STATE, "no imposed tangent resident (run pfem_newton first)");
+  cudaSetDevice(ctx->device);
+  const int prec = ctx->tangent_prec;
+  int rc;
+  bool conv = false;
+  int it = 0;
+  std::vector<double> hb(b, b + ctx->ndof);
+  if (prec == PFEM_FP64) {
+    if (rebuild_pc || !ctx->amg64.built) { rc = amg_setup<double>(ctx, o->cheb_degree); if (rc) return rc; }
+    ctx->amg64.lv[0].A.val = ctx->dK64;
+    CK(cudaMemcpy(ctx->kw64.b, hb.data(), ctx->ndof * sizeof(double), cudaMemcpyHostToDevice));
+    rc = krylov<double>(ctx, o->krylov, rtol, o->krylov_itmax, &it, &conv);
+    if (rc) return rc;
+    CK(cudaMemcpy(x, ctx->kw64.x, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  } else {
+    if (rebuild_pc || !ctx->amg32.built) { rc = amg_setup<float>(ctx, o->cheb_degree); if (rc) return rc; }
+    ctx->amg32.lv[0].A.val = ctx->dK32;
+    std::vector<float> hf(hb.begin(), hb.end());
+    CK(cudaMemcpy(ctx->kw32.b, hf.data(), ctx->ndof * sizeof(float), cudaMemcpyHostToDevice));
+    rc = krylov<float>(ctx, o->krylov, rtol, o->krylov_itmax, &it, &conv);
+    if (rc) return rc;
+    std::vector<float> xf(ctx->ndof);
+    CK(cudaMemcpy(xf.data(), ctx->kw32.x, ctx->ndof * sizeof(float), cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < ctx->ndof; ++i) x[i] = xf[i];
+  }
+  if (niter) *niter = it;
+  return conv ? PFEM_OK : fail(ctx, PFEM_ERR_LINSOLVE, "Krylov solve did not reach its tolerance");
+}
+
+int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, double* cpi, double* epsp,
+                   uint8_t* flags) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return PFEM_ERR_STATE;
+  pfem_ctx* c = const_cast<pfem_ctx*>(ctx);
+  cudaSetDevice(ctx->device);
+  if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return PFEM_ERR_CUDA;
+  const long long ngp = ctx->ngp;
+  auto soa = [&](const double* d, double* h) -> int {
+    std::vector<double> t(6 * ngp);
+    if (cudaMemcpy(t.data(), d, 6 * ngp * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+    for (long long g = 0; g < ngp; ++g)
+      for (int k = 0; k < 6; ++k) h[g * 6 + k] = t[k * ngp + g];
+    return PFEM_OK;
+  };
+  if (U && cudaMemcpy(U, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (alpha && cudaMemcpy(alpha, ctx->dAlpha, ngp * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (flags && cudaMemcpy(flags, ctx->dFlags, ngp, cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (tau && soa(ctx->dTau, tau)) return PFEM_ERR_CUDA;
+  if (cpi && soa(ctx->dCpi, cpi)) return PFEM_ERR_CUDA;
+  if (epsp && soa(ctx->dEpsp, epsp)) return PFEM_ERR_CUDA;
+  (void)c;
+  return PFEM_OK;
+}
+
+int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma) {
+  if (!ctx || !sigma) return PFEM_ERR_BAD_ARG;
+  // tau / det F at each Gauss point with the standard F (Model.jl:188-208)
+  std::vector<double> U(ctx->ndof);
+  int rc = pfem_get_state(ctx, U.data(), sigma, nullptr, nullptr, nullptr, nullptr);
+  if (rc) return rc;
+  const double gc = 1.0 / std::sqrt(3.0);
+  static const int sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
+                   sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  par_for(ctx->ne, [&](long long e) {
+    for (int g = 0; g < 8; ++g) {
+      const double xi = sx[g] * gc, et = sy[g] * gc, ze = sz[g] * gc;
+      double J[9] = {0}, H[9] = {0};
+      for (int a = 0; a < 8; ++a) {
+        const double d0 = 0.125 * sx[a] * (1 + sy[a] * et) * (1 + sz[a] * ze);
+        const double d1 = 0.125 * sy[a] * (1 + sx[a] * xi) * (1 + sz[a] * ze);
+        const double d2 = 0.125 * sz[a] * (1 + sx[a] * xi) * (1 + sy[a] * et);
+        const int n = ctx->elem[e * 8 + a];
+        for (int i = 0; i < 3; ++i) {
+          J[3 * i] += ctx->X[n * 3 + i] * d0; J[3 * i + 1] += ctx->X[n * 3 + i] * d1; J[3 * i + 2] += ctx->X[n * 3 + i] * d2;
+          H[3 * i] += U[n * 3 + i] * d0; H[3 * i + 1] += U[n * 3 + i] * d1; H[3 * i + 2] += U[n * 3 + i] * d2;
+        }
+      }
+      const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+      double Ji[9];
+      Ji[0] = (J[4] * J[8] - J[5] * J[7]) / dJ; Ji[1] = (J[2] * J[7] - J[1] * J[8]) / dJ; Ji[2] = (J[1] * J[5] - J[2] * J[4]) / dJ;
+      Ji[3] = (J[5] * J[6] - J[3] * J[8]) / dJ; Ji[4] = (J[0] * J[8] - J[2] * J[6]) / dJ; Ji[5] = (J[2] * J[3] - J[0] * J[5]) / dJ;
+      Ji[6] = (J[3] * J[7] - J[4] * J[6]) / dJ; Ji[7] = (J[1] * J[6] - J[0] * J[7]) / dJ; Ji[8] = (J[0] * J[4] - J[1] * J[3]) / dJ;
+      double F[9];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          F[3 * i + j] = (i == j ? 1.0 : 0.0) + H[3 * i] * Ji[j] + H[3 * i + 1] * Ji[3 + j] + H[3 * i + 2] * Ji[6 + j];
+      const double dF = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) + F[2] * (F[3] * F[7] - F[4] * F[6]);
+      const double inv = dF > 0 ? 1.0 / dF : 1.0;
+      for (int k = 0; k < 6; ++k) sigma[(e * 8 + g) * 6 + k] *= inv;
+    }
+  });
+  return PFEM_OK;
+}
+
+int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms) {
+  if (!ctx || !ms || reps <= 0) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc;
+  if (what == 0 || what == 1) {
+    const int prec = what == 0 ? PFEM_FP64 : PFEM_MIXED;
+    rc = ensure_tangent(ctx, prec);
+    if (rc) return rc;
+    rc = assemble_dev(ctx, prec, false);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->e0, ctx->st));
+    for (int i = 0; i < reps; ++i) {
+      rc = assemble_dev(ctx, prec, false);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(ctx->e1, ctx->st));
+  } else if (what == 2 || what == 3) {
+    if (!ctx->amg_struct) build_amg_structure(ctx);
+    if (what == 2) {
+      rc = ensure_tangent(ctx, PFEM_MIXED); if (rc) return rc;
+      rc = amg_alloc<float>(ctx); if (rc) return rc;
+      rc = krylov_alloc<float>(ctx); if (rc) return rc;
+      BsrMat<float> A = ctx->amg32.lv[0].A;
+      A.val = ctx->dK32;
+      fill<float>(ctx->ndof, ctx->kw32.p, 1.0f, ctx->st);
+      bsr_spmv<float>(A, ctx->kw32.p, ctx->kw32.q, ctx->st);
+      CK(cudaEventRecord(ctx->e0, ctx->st));
+      for (int i = 0; i < reps; ++i) bsr_spmv<float>(A, ctx->kw32.p, ctx->kw32.q, ctx->st);
+      CK(cudaEventRecord(ctx->e1, ctx->st));
+    } else {
+      rc = ensure_tangent(ctx, PFEM_FP64); if (rc) return rc;
+      rc = amg_alloc<double>(ctx); if (rc) return rc;
+      rc = krylov_alloc<double>(ctx); if (rc) return rc;
+      BsrMat<double> A = ctx->amg64.lv[0].A;
+      A.val = ctx->dK64;
+      fill<double>(ctx->ndof, ctx->kw64.p, 1.0, ctx->st);
+      bsr_spmv<double>(A, ctx->kw64.p, ctx->kw64.q, ctx->st);
+      CK(cudaEventRecord(ctx->e0, ctx->st));
+      for (int i = 0; i < reps; ++i) bsr_spmv<double>(A, ctx->kw64.p, ctx->kw64.q, ctx->st);
+      CK(cudaEventRecord(ctx->e1, ctx->st));
+    }
+  } else {
+    return PFEM_ERR_BAD_ARG;
+  }
+  CKL();
+  CK(cudaEventSynchronize(ctx->e1));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, ctx->e0, ctx->e1));
+  *ms = t / reps;
+  return PFEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,559 @@
+// linalg.cu -- block-CSR SpMV, smoother / Krylov vector kernels, reductions,
+// Dirichlet imposition and AMG transfer kernels.  All are HBM-bound; each is
+// written so that one pass over the matrix does all the work the caller needs
+// from that pass (SpMV + residual, SpMV + block-Jacobi Chebyshev update).
+#include "linalg.cuh"
+
+namespace pfem {
+
+// ------------------------------------------------------------------ SpMV
+// One warp per block row; lane k holds block rowptr[i]+k (+32, ...), loads the
+// whole bs x bs block and the matching bs entries of x, and the warp reduces
+// the bs partial sums.  Mode selects the epilogue:
+//   0: y = A x
+//   1: y = b - A x                          (residual)
+//   2: r -= Dinv (A x); xo += x             (Chebyshev step on x = d)
+template <typename T, int BS, int MODE>
+__global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __restrict__ rowptr,
+                                                       const int* __restrict__ col,
+                                                       const T* __restrict__ val,
+                                                       const T* __restrict__ x, T* __restrict__ y,
+                                                       const T* __restrict__ b,
+                                                       const T* __restrict__ dinv, T* __restrict__ xo) {
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nbrow) return;
+  const int s = rowptr[row], e = rowptr[row + 1];
+  T acc[BS];
+#pragma unroll
+  for (int i = 0; i < BS; ++i) acc[i] = T(0);
+  for (int k = s + lane; k < e; k += 32) {
+    const int c = col[k];
+    const T* B = val + (long long)k * (BS * BS);
+    T xv[BS];
+#pragma unroll
+    for (int j = 0; j < BS; ++j) xv[j] = x[(long long)c * BS + j];
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int j = 0; j < BS; ++j) acc[i] += B[i * BS + j] * xv[j];
+  }
+#pragma unroll
+  for (int i = 0; i < BS; ++i) {
+    T v = acc[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    acc[i] = v;
+  }
+  if (lane < BS) {
+    const long long base = (long long)row * BS;
+    T v = acc[0];
+#pragma unroll
+    for (int i = 1; i < BS; ++i)
+      if (lane == i) v = acc[i];
+    if (MODE == 0) {
+      y[base + lane] = v;
+    } else if (MODE == 1) {
+      y[base + lane] = b[base + lane] - v;
+    } else {
+      // r_i -= Dinv_i (A d)_i  (row lane of the bs x bs block product)
+      const T* D = dinv + (long long)row * (BS * BS);
+      T t = T(0);
+#pragma unroll
+      for (int j = 0; j < BS; ++j) t += D[lane * BS + j] * acc[j];
+      y[base + lane] -= t;
+      xo[base + lane] += x[base + lane];
+    }
+  }
+}
+
+template <typename T>
+void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st) {
+  const long long threads = (long long)A.nbrow * 32;
+  const int blocks = (int)((threads + 255) / 256);
+  if (A.bs == 3)
+    bsr_spmv_kernel<T, 3, 0><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, nullptr, nullptr, nullptr);
+  else
+    bsr_spmv_kernel<T, 6, 0><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, nullptr, nullptr, nullptr);
+}
+template <typename T>
+void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t st) {
+  const long long threads = (long long)A.nbrow * 32;
+  const int blocks = (int)((threads + 255) / 256);
+  if (A.bs == 3)
+    bsr_spmv_kernel<T, 3, 1><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, r, b, nullptr, nullptr);
+  else
+    bsr_spmv_kernel<T, 6, 1><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, r, b, nullptr, nullptr);
+}
+template <typename T>
+void bsr_cheb_step(const BsrMat<T>& A, const T* dinv, const T* d, T* r, T* x, cudaStream_t st) {
+  const long long threads = (long long)A.nbrow * 32;
+  const int blocks = (int)((threads + 255) / 256);
+  if (A.bs == 3)
+    bsr_spmv_kernel<T, 3, 2><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, d, r, nullptr, dinv, x);
+  else
+    bsr_spmv_kernel<T, 6, 2><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, d, r, nullptr, dinv, x);
+}
+
+// ------------------------------------------------------------------ block diagonal
+// r = Dinv * v per block row (one thread per scalar row); optional scale.
+template <typename T, int BS>
+__global__ void blockdiag_apply_kernel(int nbrow, const T* __restrict__ dinv, const T* __restrict__ v,
+                                       T* __restrict__ r, T scale, T* __restrict__ d) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nbrow * BS) return;
+  const long long row = i / BS;
+  const int li = (int)(i - row * BS);
+  const T* D = dinv + row * (BS * BS) + li * BS;
+  const T* vv = v + row * BS;
+  T t = T(0);
+#pragma unroll
+  for (int j = 0; j < BS; ++j) t += D[j] * vv[j];
+  r[i] = t;
+  if (d) d[i] = scale * t;
+}
+template <typename T>
+void blockdiag_apply(int nbrow, int bs, const T* dinv, const T* v, T* r, T scale, T* d, cudaStream_t st) {
+  const long long n = (long long)nbrow * bs;
+  const int blocks = (int)((n + 255) / 256);
+  if (bs == 3) blockdiag_apply_kernel<T, 3><<<blocks, 256, 0, st>>>(nbrow, dinv, v, r, scale, d);
+  else blockdiag_apply_kernel<T, 6><<<blocks, 256, 0, st>>>(nbrow, dinv, v, r, scale, d);
+}
+
+// Invert the diagonal blocks (Gauss-Jordan with partial pivoting in double).
+// A singular block (a Dirichlet-free rigid aggregate, say) gets the inverse of
+// its diagonal instead, with zero diagonal entries mapped to 1.
+template <typename T, int BS>
+__global__ void blockdiag_invert_kernel(int nbrow, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                        const T* __restrict__ val, T* __restrict__ dinv) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nbrow) return;
+  double a[BS][2 * BS];
+  int kd = -1;
+  for (int k = rowptr[row]; k < rowptr[row + 1]; ++k)
+    if (col[k] == row) { kd = k; break; }
+  for (int i = 0; i < BS; ++i)
+    for (int j = 0; j < BS; ++j) {
+      a[i][j] = kd >= 0 ? (double)val[(long long)kd * BS * BS + i * BS + j] : 0.0;
+      a[i][BS + j] = (i == j) ? 1.0 : 0.0;
+    }
+  bool ok = true;
+  double scl = 0.0;
+  for (int i = 0; i < BS; ++i) scl = fmax(scl, fabs(a[i][i]));
+  for (int c = 0; c < BS && ok; ++c) {
+    int piv = c;
+    double best = fabs(a[c][c]);
+    for (int r = c + 1; r < BS; ++r)
+      if (fabs(a[r][c]) > best) { best = fabs(a[r][c]); piv = r; }
+    if (!(best > 1e-13 * scl) || !(best > 0.0)) { ok = false; break; }
+    if (piv != c)
+      for (int j = 0; j < 2 * BS; ++j) { double t = a[c][j]; a[c][j] = a[piv][j]; a[piv][j] = t; }
+    const double ip = 1.0 / a[c][c];
+    for (int j = 0; j < 2 * BS; ++j) a[c][j] *= ip;
+    for (int r = 0; r < BS; ++r)
+      if (r != c) {
+        const double f = a[r][c];
+        if (f != 0.0)
+          for (int j = 0; j < 2 * BS; ++j) a[r][j] -= f * a[c][j];
+      }
+  }
+  T* D = dinv + (long long)row * BS * BS;
+  if (ok) {
+    for (int i = 0; i < BS; ++i)
+      for (int j = 0; j < BS; ++j) D[i * BS + j] = (T)a[i][BS + j];
+  } else {
+    for (int i = 0; i < BS; ++i)
+      for (int j = 0; j < BS; ++j) {
+        double dv = kd >= 0 ? (double)val[(long long)kd * BS * BS + i * BS + i] : 0.0;
+        D[i * BS + j] = (i == j) ? (T)(dv != 0.0 ? 1.0 / dv : 1.0) : T(0);
+      }
+  }
+}
+template <typename T>
+void blockdiag_invert(const BsrMat<T>& A, T* dinv, cudaStream_t st) {
+  const int blocks = (A.nbrow + 127) / 128;
+  if (A.bs == 3) blockdiag_invert_kernel<T, 3><<<blocks, 128, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, dinv);
+  else blockdiag_invert_kernel<T, 6><<<blocks, 128, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, dinv);
+}
+
+// ------------------------------------------------------------------ reductions
+// Deterministic two-pass dot product: per-block partials, then one block.
+constexpr int RED_THREADS = 256;
+constexpr int RED_BLOCKS = 1184;  // 148 SMs x 8
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : T(0);
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+template <typename T>
+__global__ void dot_partial_kernel(long long n, const T* __restrict__ a, const T* __restrict__ b,
+                                   T* __restrict__ part) {
+  __shared__ T sh[32];
+  T v = T(0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    v += a[i] * b[i];
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+template <typename T>
+__global__ void sum_final_kernel(int np, const T* __restrict__ part, T* __restrict__ out, int sqrt_out) {
+  __shared__ T sh[32];
+  T v = T(0);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) *out = sqrt_out ? sqrt(v) : v;
+}
+template <typename T>
+void dot(long long n, const T* a, const T* b, T* out, T* part, cudaStream_t st, bool take_sqrt) {
+  long long nb = (n + RED_THREADS - 1) / RED_THREADS;
+  const int blocks = (int)(nb < RED_BLOCKS ? (nb > 0 ? nb : 1) : RED_BLOCKS);
+  dot_partial_kernel<T><<<blocks, RED_THREADS, 0, st>>>(n, a, b, part);
+  sum_final_kernel<T><<<1, 1024, 0, st>>>(blocks, part, out, take_sqrt ? 1 : 0);
+}
+
+// ------------------------------------------------------------------ vector ops
+template <typename T>
+__global__ void fill_kernel(long long n, T* x, T v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+template <typename T>
+void fill(long long n, T* x, T v, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  if (n > 0) fill_kernel<T><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(n, x, v);
+}
+// y = a*x + b*y with host scalars
+template <typename T>
+__global__ void axpby_kernel(long long n, T a, const T* __restrict__ x, T b, T* __restrict__ y) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
+}
+template <typename T>
+void axpby(long long n, T a, const T* x, T b, T* y, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  if (n > 0) axpby_kernel<T><<<blocks, 256, 0, st>>>(n, a, x, b, y);
+}
+// CG update with device scalars: alpha = num/den;  x += alpha p;  r -= alpha q
+template <typename T>
+__global__ void cg_xr_kernel(long long n, const T* __restrict__ num, const T* __restrict__ den,
+                             const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
+                             T* __restrict__ r) {
+  const T al = *num / *den;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += al * p[i];
+    r[i] -= al * q[i];
+  }
+}
+template <typename T>
+void cg_xr(long long n, const T* num, const T* den, const T* p, const T* q, T* x, T* r, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  cg_xr_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, p, q, x, r);
+}
+// p = z + (num/den) p
+template <typename T>
+__global__ void cg_p_kernel(long long n, const T* __restrict__ num, const T* __restrict__ den,
+                            const T* __restrict__ z, T* __restrict__ p) {
+  const T be = *num / *den;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = z[i] + be * p[i];
+}
+template <typename T>
+void cg_p(long long n, const T* num, const T* den, const T* z, T* p, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  cg_p_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, z, p);
+}
+// BiCGStab helpers with device scalars s[0..]: see krylov code for layout.
+template <typename T>
+__global__ void bicg_p_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ r,
+                              const T* __restrict__ v, T* __restrict__ p) {
+  // beta = (rho_new/rho_old)*(alpha/omega); p = r + beta (p - omega v)
+  const T beta = (sc[0] / sc[1]) * (sc[2] / sc[3]);
+  const T om = sc[3];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = r[i] + beta * (p[i] - om * v[i]);
+}
+template <typename T>
+void bicg_p(long long n, const T* sc, const T* r, const T* v, T* p, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  bicg_p_kernel<T><<<blocks, 256, 0, st>>>(n, sc, r, v, p);
+}
+// s = r - alpha v  (alpha = sc[0]/sc[4])
+template <typename T>
+__global__ void bicg_s_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ r,
+                              const T* __restrict__ v, T* __restrict__ s) {
+  const T al = sc[0] / sc[4];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s[i] = r[i] - al * v[i];
+}
+template <typename T>
+void bicg_s(long long n, const T* sc, const T* r, const T* v, T* s, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  bicg_s_kernel<T><<<blocks, 256, 0, st>>>(n, sc, r, v, s);
+}
+// x += alpha ph + omega sh;  r = s - omega t  (alpha = sc[0]/sc[4], omega = sc[5]/sc[6])
+template <typename T>
+__global__ void bicg_xr_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ ph,
+                               const T* __restrict__ sh, const T* __restrict__ s, const T* __restrict__ t,
+                               T* __restrict__ x, T* __restrict__ r) {
+  const T al = sc[0] / sc[4];
+  const T om = sc[5] / sc[6];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += al * ph[i] + om * sh[i];
+    r[i] = s[i] - om * t[i];
+  }
+}
+template <typename T>
+void bicg_xr(long long n, const T* sc, const T* ph, const T* sh, const T* s, const T* t, T* x, T* r,
+             cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  bicg_xr_kernel<T><<<blocks, 256, 0, st>>>(n, sc, ph, sh, s, t, x, r);
+}
+// scalar bookkeeping: dst[i] = src[j]
+template <typename T>
+__global__ void scalar_copy_kernel(T* dst, const T* src) { *dst = *src; }
+template <typename T>
+void scalar_copy(T* dst, const T* src, cudaStream_t st) { scalar_copy_kernel<T><<<1, 1, 0, st>>>(dst, src); }
+
+// precision conversion
+template <typename A, typename B>
+__global__ void convert_kernel(long long n, const A* __restrict__ a, B* __restrict__ b, double s) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (B)(s * (double)a[i]);
+}
+template <typename A, typename B>
+void convert(long long n, const A* a, B* b, double s, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  convert_kernel<A, B><<<blocks, 256, 0, st>>>(n, a, b, s);
+}
+// U += (double) x
+template <typename T>
+__global__ void add_to_double_kernel(long long n, const T* __restrict__ x, double* __restrict__ U) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    U[i] += (double)x[i];
+}
+template <typename T>
+void add_to_double(long long n, const T* x, double* U, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  add_to_double_kernel<T><<<blocks, 256, 0, st>>>(n, x, U);
+}
+
+// ------------------------------------------------------------------ Dirichlet (K3)
+// R -= lambda * Fn  over all dofs, then dg = g(lambda) - U on constrained dofs.
+__global__ void residual_fext_kernel(long long n, double lam, const double* __restrict__ fn,
+                                     double* __restrict__ R) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    R[i] -= lam * fn[i];
+}
+__global__ void bc_dg_kernel(int nbc, const int* __restrict__ dofs, const double* __restrict__ vals,
+                             const uint8_t* __restrict__ ramp, double lam, const double* __restrict__ U,
+                             double* __restrict__ dg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbc) return;
+  const int d = dofs[i];
+  const double g = ramp[i] ? lam * vals[i] : vals[i];
+  dg[d] = g - U[d];
+}
+// Free rows touching constrained columns: R[row] += sum_k K[pos_k] * dg[col_k]
+// (impose_dirichlet!, BoundaryConditions.jl:248-256).  One thread per row.
+template <typename KT>
+__global__ void bc_rhs_kernel(int nrows, const int* __restrict__ rows, const int* __restrict__ ptr,
+                              const long long* __restrict__ pos, const int* __restrict__ cols,
+                              const KT* __restrict__ K, const double* __restrict__ dg,
+                              double* __restrict__ R) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nrows) return;
+  double s = 0.0;
+  for (int k = ptr[i]; k < ptr[i + 1]; ++k) s += (double)K[pos[k]] * dg[cols[k]];
+  R[rows[i]] += s;
+}
+// Zero constrained rows / columns, unit diagonal (BoundaryConditions.jl:259-266).
+template <typename KT>
+__global__ void bc_zero_kernel(long long n, const long long* __restrict__ pos, const uint8_t* __restrict__ one,
+                               KT* __restrict__ K) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    K[pos[i]] = one[i] ? KT(1) : KT(0);
+}
+// R[d] = -dg[d] (BoundaryConditions.jl:269-272)
+__global__ void bc_set_kernel(int nbc, const int* __restrict__ dofs, const double* __restrict__ dg,
+                              double* __restrict__ R) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbc) return;
+  R[dofs[i]] = -dg[dofs[i]];
+}
+template <typename KT>
+void impose_dirichlet(const BcDev& bc, long long ndof, double lam, const double* U, KT* K, double* R,
+                      double* dg, cudaStream_t st) {
+  const int b1 = (int)std::min<long long>((ndof + 255) / 256, 4096);
+  residual_fext_kernel<<<b1, 256, 0, st>>>(ndof, lam, bc.fn, R);
+  if (bc.nbc == 0) return;
+  bc_dg_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U, dg);
+  if (bc.nrows > 0)
+    bc_rhs_kernel<KT><<<(bc.nrows + 127) / 128, 128, 0, st>>>(bc.nrows, bc.rows, bc.rptr, bc.rpos, bc.rcol, K, dg, R);
+  if (bc.nzero > 0) {
+    const int b2 = (int)std::min<long long>((bc.nzero + 255) / 256, 4096);
+    bc_zero_kernel<KT><<<b2, 256, 0, st>>>(bc.nzero, bc.zpos, bc.zone, K);
+  }
+  bc_set_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, dg, R);
+}
+// Set U[d] = g(lambda) on constrained dofs (predictors honour the BCs).
+__global__ void bc_apply_kernel(int nbc, const int* __restrict__ dofs, const double* __restrict__ vals,
+                                const uint8_t* __restrict__ ramp, double lam, double* __restrict__ U) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbc) return;
+  U[dofs[i]] = ramp[i] ? lam * vals[i] : vals[i];
+}
+void bc_apply(const BcDev& bc, double lam, double* U, cudaStream_t st) {
+  if (bc.nbc > 0) bc_apply_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U);
+}
+
+// ------------------------------------------------------------------ AMG transfer
+// Galerkin product with the tentative prolongator: for every fine block
+// (n, m):  C += T_n^T A_nm T_m  into coarse block f2c[k] (6 x 6).
+template <typename T, int BS>
+__global__ void galerkin_kernel(int nbrow, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                const T* __restrict__ val, const T* __restrict__ Tb,
+                                const int* __restrict__ f2c, T* __restrict__ cval) {
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nbrow) return;
+  const T* Tn = Tb + (long long)row * BS * 6;
+  for (int k = rowptr[row] + lane; k < rowptr[row + 1]; k += 32) {
+    const int m = col[k];
+    const T* A = val + (long long)k * BS * BS;
+    const T* Tm = Tb + (long long)m * BS * 6;
+    T W[BS][6];
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < BS; ++j) s += A[i * BS + j] * Tm[j * 6 + c];
+        W[i][c] = s;
+      }
+    T* C = cval + (long long)f2c[k] * 36;
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        T s = T(0);
+#pragma unroll
+        for (int i = 0; i < BS; ++i) s += Tn[i * 6 + r] * W[i][c];
+        atomicAdd(C + r * 6 + c, s);
+      }
+  }
+}
+template <typename T>
+void galerkin(const BsrMat<T>& A, const T* Tb, const int* f2c, T* cval, cudaStream_t st) {
+  const long long threads = (long long)A.nbrow * 32;
+  const int blocks = (int)((threads + 255) / 256);
+  if (A.bs == 3) galerkin_kernel<T, 3><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, Tb, f2c, cval);
+  else galerkin_kernel<T, 6><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, Tb, f2c, cval);
+}
+// Restriction: bc[I*6 + c] = sum_{n in I} (T_n^T r_n)_c
+template <typename T, int BS>
+__global__ void restrict_kernel(int nagg, const int* __restrict__ aptr, const int* __restrict__ amem,
+                                const T* __restrict__ Tb, const T* __restrict__ r, T* __restrict__ bc) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nagg * 6) return;
+  const int I = (int)(i / 6), c = (int)(i % 6);
+  T s = T(0);
+  for (int k = aptr[I]; k < aptr[I + 1]; ++k) {
+    const int n = amem[k];
+    const T* Tn = Tb + (long long)n * BS * 6;
+#pragma unroll
+    for (int j = 0; j < BS; ++j) s += Tn[j * 6 + c] * r[(long long)n * BS + j];
+  }
+  bc[i] = s;
+}
+template <typename T>
+void amg_restrict(int nagg, int bs, const int* aptr, const int* amem, const T* Tb, const T* r, T* bc, cudaStream_t st) {
+  const long long n = (long long)nagg * 6;
+  const int blocks = (int)((n + 255) / 256);
+  if (bs == 3) restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(nagg, aptr, amem, Tb, r, bc);
+  else restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(nagg, aptr, amem, Tb, r, bc);
+}
+// Prolongation: x_n += T_n xc[agg(n)]
+template <typename T, int BS>
+__global__ void prolong_kernel(int nbrow, const int* __restrict__ agg, const T* __restrict__ Tb,
+                               const T* __restrict__ xc, T* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nbrow * BS) return;
+  const long long n = i / BS;
+  const int j = (int)(i - n * BS);
+  const T* Tn = Tb + n * BS * 6 + j * 6;
+  const T* xa = xc + (long long)agg[n] * 6;
+  T s = T(0);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) s += Tn[c] * xa[c];
+  x[i] += s;
+}
+template <typename T>
+void amg_prolong(int nbrow, int bs, const int* agg, const T* Tb, const T* xc, T* x, cudaStream_t st) {
+  const long long n = (long long)nbrow * bs;
+  const int blocks = (int)((n + 255) / 256);
+  if (bs == 3) prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(nbrow, agg, Tb, xc, x);
+  else prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(nbrow, agg, Tb, xc, x);
+}
+// Dense coarse solve y = Ainv b (one warp per row).
+template <typename T>
+__global__ void dense_mv_kernel(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ y) {
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  T s = T(0);
+  for (int j = lane; j < n; j += 32) s += M[(long long)row * n + j] * b[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] = s;
+}
+template <typename T>
+void dense_mv(int n, const T* M, const T* b, T* y, cudaStream_t st) {
+  const int blocks = (int)(((long long)n * 32 + 255) / 256);
+  dense_mv_kernel<T><<<blocks, 256, 0, st>>>(n, M, b, y);
+}
+
+// ------------------------------------------------------------------ instantiations
+#define PFEM_INST(T)                                                                               \
+  template void bsr_spmv<T>(const BsrMat<T>&, const T*, T*, cudaStream_t);                         \
+  template void bsr_residual<T>(const BsrMat<T>&, const T*, const T*, T*, cudaStream_t);           \
+  template void bsr_cheb_step<T>(const BsrMat<T>&, const T*, const T*, T*, T*, cudaStream_t);      \
+  template void blockdiag_apply<T>(int, int, const T*, const T*, T*, T, T*, cudaStream_t);         \
+  template void blockdiag_invert<T>(const BsrMat<T>&, T*, cudaStream_t);                           \
+  template void dot<T>(long long, const T*, const T*, T*, T*, cudaStream_t, bool);                 \
+  template void fill<T>(long long, T*, T, cudaStream_t);                                           \
+  template void axpby<T>(long long, T, const T*, T, T*, cudaStream_t);                             \
+  template void cg_xr<T>(long long, const T*, const T*, const T*, const T*, T*, T*, cudaStream_t); \
+  template void cg_p<T>(long long, const T*, const T*, const T*, T*, cudaStream_t);                \
+  template void bicg_p<T>(long long, const T*, const T*, const T*, T*, cudaStream_t);              \
+  template void bicg_s<T>(long long, const T*, const T*, const T*, T*, cudaStream_t);              \
+  template void bicg_xr<T>(long long, const T*, const T*, const T*, const T*, const T*, T*, T*,    \
+                           cudaStream_t);                                                          \
+  template void scalar_copy<T>(T*, const T*, cudaStream_t);                                        \
+  template void add_to_double<T>(long long, const T*, double*, cudaStream_t);                      \
+  template void impose_dirichlet<T>(const BcDev&, long long, double, const double*, T*, double*,   \
+                                    double*, cudaStream_t);                                        \
+  template void galerkin<T>(const BsrMat<T>&, const T*, const int*, T*, cudaStream_t);             \
+  template void amg_restrict<T>(int, int, const int*, const int*, const T*, const T*, T*,          \
+                                cudaStream_t);                                                     \
+  template void amg_prolong<T>(int, int, const int*, const T*, const T*, T*, cudaStream_t);        \
+  template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);
+PFEM_INST(float)
+PFEM_INST(double)
+template void convert<double, float>(long long, const double*, float*, double, cudaStream_t);
+template void convert<float, double>(long long, const float*, double*, double, cudaStream_t);
+template void convert<double, double>(long long, const double*, double*, double, cudaStream_t);
+
+}  // namespace pfem

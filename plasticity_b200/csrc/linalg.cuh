@@ -1,0 +1,49 @@
+// linalg.cuh -- declarations of the solver-side kernels (linalg.cu).
+#pragma once
+#include <algorithm>
+#include "pfem_internal.h"
+
+namespace pfem {
+
+// Device copy of the frozen boundary conditions plus the precomputed list of
+// tangent entries that Dirichlet imposition reads and overwrites.
+struct BcDev {
+  int nbc = 0;                 // constrained dofs (deduplicated)
+  int* dofs = nullptr;         // 0-based dof
+  double* vals = nullptr;
+  uint8_t* ramp = nullptr;
+  double* fn = nullptr;        // ndof nodal forces at lambda = 1
+  int nrows = 0;               // free rows with entries in constrained columns
+  int* rows = nullptr;
+  int* rptr = nullptr;         // nrows+1
+  long long* rpos = nullptr;   // scalar value index into the block-CSR value array
+  int* rcol = nullptr;         // constrained column (dof)
+  long long nzero = 0;         // entries in constrained rows or columns
+  long long* zpos = nullptr;
+  uint8_t* zone = nullptr;     // 1 on the diagonal of a constrained row
+};
+
+template <typename T> void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st);
+template <typename T> void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t st);
+template <typename T> void bsr_cheb_step(const BsrMat<T>& A, const T* dinv, const T* d, T* r, T* x, cudaStream_t st);
+template <typename T> void blockdiag_apply(int nbrow, int bs, const T* dinv, const T* v, T* r, T scale, T* d, cudaStream_t st);
+template <typename T> void blockdiag_invert(const BsrMat<T>& A, T* dinv, cudaStream_t st);
+template <typename T> void dot(long long n, const T* a, const T* b, T* out, T* part, cudaStream_t st, bool take_sqrt);
+template <typename T> void fill(long long n, T* x, T v, cudaStream_t st);
+template <typename T> void axpby(long long n, T a, const T* x, T b, T* y, cudaStream_t st);
+template <typename T> void cg_xr(long long n, const T* num, const T* den, const T* p, const T* q, T* x, T* r, cudaStream_t st);
+template <typename T> void cg_p(long long n, const T* num, const T* den, const T* z, T* p, cudaStream_t st);
+template <typename T> void bicg_p(long long n, const T* sc, const T* r, const T* v, T* p, cudaStream_t st);
+template <typename T> void bicg_s(long long n, const T* sc, const T* r, const T* v, T* s, cudaStream_t st);
+template <typename T> void bicg_xr(long long n, const T* sc, const T* ph, const T* sh, const T* s, const T* t, T* x, T* r, cudaStream_t st);
+template <typename T> void scalar_copy(T* dst, const T* src, cudaStream_t st);
+template <typename A, typename B> void convert(long long n, const A* a, B* b, double s, cudaStream_t st);
+template <typename T> void add_to_double(long long n, const T* x, double* U, cudaStream_t st);
+template <typename KT> void impose_dirichlet(const BcDev& bc, long long ndof, double lam, const double* U, KT* K, double* R, double* dg, cudaStream_t st);
+void bc_apply(const BcDev& bc, double lam, double* U, cudaStream_t st);
+template <typename T> void galerkin(const BsrMat<T>& A, const T* Tb, const int* f2c, T* cval, cudaStream_t st);
+template <typename T> void amg_restrict(int nagg, int bs, const int* aptr, const int* amem, const T* Tb, const T* r, T* bc, cudaStream_t st);
+template <typename T> void amg_prolong(int nbrow, int bs, const int* agg, const T* Tb, const T* xc, T* x, cudaStream_t st);
+template <typename T> void dense_mv(int n, const T* M, const T* b, T* y, cudaStream_t st);
+
+}  // namespace pfem

@@ -1,0 +1,76 @@
+// pfem_internal.h -- device-side data structures shared by the CUDA sources.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "../../include/pfem_b200.h"
+
+namespace pfem {
+
+template <typename KT>
+struct ElemArgs {
+  const double* X;         // nn x 3 node coordinates (node-major)
+  const int* elem;         // ne x 8 node ids (0-based)
+  const double* U;         // ndof displacements
+  double* cpi;             // 6 x ngp committed Cp^-1 (component-major SoA)
+  double* alpha;           // ngp committed equivalent plastic strain
+  double* epsp;            // 6 x ngp accumulated plastic strain (diagnostic)
+  const double* sigy0_e;   // ne per-element initial yield stress, or null
+  double* tau;             // 6 x ngp Kirchhoff stress of the last evaluation
+  uint8_t* flags;          // ngp elastic(0)/plastic(1) of the last evaluation
+  double* R;               // ndof internal force (accumulated)
+  KT* Kval;                // nnzb x 9 block-CSR tangent values (accumulated)
+  const int* browptr;      // nn+1 block row pointers
+  const uint8_t* rank;     // ne x 64: position of node b in node a's block row
+  long long ngp;
+  MatParams mat;
+  DevStatus* status;
+};
+
+template <typename KT>
+void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit, bool fbar,
+                          cudaStream_t st);
+size_t element_smem_bytes();
+
+// ---------------- block-CSR matrices ----------------
+template <typename VT>
+struct BsrMat {
+  int nbrow = 0;     // block rows (== block cols)
+  int bs = 0;        // block size
+  long long nnzb = 0;
+  int* rowptr = nullptr;  // device, nbrow+1
+  int* col = nullptr;     // device, nnzb
+  VT* val = nullptr;      // device, nnzb*bs*bs (row-major blocks)
+};
+
+// One AMG level.  P is the tentative prolongator of aggregation-based AMG:
+// every fine block row n belongs to exactly one aggregate agg[n] and carries
+// a dense bs x 6 block T_n.
+template <typename VT>
+struct AmgLevel {
+  BsrMat<VT> A;
+  VT* dinv = nullptr;     // nbrow x bs x bs inverse diagonal blocks
+  VT lmax = 0;            // spectral radius estimate of D^-1 A
+  int nagg = 0;
+  int* agg = nullptr;     // nbrow aggregate of each block row
+  VT* T = nullptr;        // nbrow x bs x 6
+  int* agg_ptr = nullptr; // nagg+1 members of each aggregate (CSR)
+  int* agg_mem = nullptr;
+  int* fine2coarse = nullptr;  // per fine block: index of the coarse block it feeds
+  // work vectors (length nbrow*bs)
+  VT *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
+};
+
+template <typename VT>
+struct Amg {
+  std::vector<AmgLevel<VT>> lv;
+  int coarse_n = 0;          // dofs of the coarsest level
+  VT* coarse_inv = nullptr;  // coarse_n x coarse_n dense inverse (row-major)
+  VT *cx = nullptr, *cb = nullptr;
+  bool built = false;
+  int cheb_degree = 2;
+};
+
+}  // namespace pfem

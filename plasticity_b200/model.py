@@ -1,0 +1,386 @@
+"""Host-side mirror of the reference's public API (lagrangian/src/PlasticityFEM.jl:35-47).
+
+Names and argument meanings follow the Julia package: ``box_mesh``, ``on_face``,
+``select_nodes``, ``J2Material``, ``Model``, ``fix``/``prescribe``/``load``
+(Julia ``fix!``/``prescribe!``/``load!``), ``solve`` (``solve!``), ``reset``,
+``nodal_displacements``, ``gauss_stress``, ``gauss_kirchhoff``,
+``equivalent_plastic_strain``, ``assemble`` (``assemble!``).  Every numerical
+call goes through the C ABI of ``libpfem_b200.so``; this module only moves
+host arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib as L
+from ._lib import check, ptr
+
+
+# ------------------------------------------------------------------ mesh (Mesh.jl)
+@dataclass
+class Mesh:
+    """Mesh (Mesh.jl:17-22): nodes 3 x nn (float64), elements 8 x ne (1-based int64)."""
+    nodes: np.ndarray
+    elements: np.ndarray
+
+    @property
+    def nnodes(self) -> int:
+        return self.nodes.shape[1]
+
+    @property
+    def nelem(self) -> int:
+        return self.elements.shape[1]
+
+
+def box_mesh(lx, ly, lz, nx: int, ny: int, nz: int) -> Mesh:
+    """box_mesh (Mesh.jl:30-59): lexicographic nodes (x fastest), VTK Hex8 order."""
+    npx, npy = nx + 1, ny + 1
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    nodes = np.stack([float(lx) * i.ravel() / nx, float(ly) * j.ravel() / ny,
+                      float(lz) * k.ravel() / nz]).astype(np.float64)
+    ke, je, ie = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ie, je, ke = ie.ravel(), je.ravel(), ke.ravel()
+
+    def nid(i, j, k):
+        return (k * npy + j) * npx + i + 1
+
+    el = np.stack([nid(ie, je, ke), nid(ie + 1, je, ke), nid(ie + 1, je + 1, ke),
+                   nid(ie, je + 1, ke), nid(ie, je, ke + 1), nid(ie + 1, je, ke + 1),
+                   nid(ie + 1, je + 1, ke + 1), nid(ie, je + 1, ke + 1)]).astype(np.int64)
+    return Mesh(nodes, el)
+
+
+def select_nodes(mesh: Mesh, pred) -> np.ndarray:
+    """select_nodes (Mesh.jl:66-74): 1-based ids where pred(x, y, z) holds."""
+    x, y, z = mesh.nodes
+    mask = np.asarray(pred(x, y, z), dtype=bool)
+    return np.nonzero(mask)[0].astype(np.int64) + 1
+
+
+def on_face(mesh: Mesh, face: str) -> np.ndarray:
+    """on_face (Mesh.jl:82-104), tolerance 1e-8 * max(L, 1)."""
+    face = face.lstrip(":")
+    x, y, z = mesh.nodes
+    lo = mesh.nodes.min(axis=1)
+    hi = mesh.nodes.max(axis=1)
+    Lmax = float(np.max(hi - lo))
+    tol = 1e-8 * max(Lmax, 1.0)
+    ax = {"x": 0, "y": 1, "z": 2}[face[0]]
+    v = lo[ax] if face.endswith("min") else hi[ax]
+    if not (face.endswith("min") or face.endswith("max")):
+        raise ValueError(f"unknown face {face}")
+    return np.nonzero(np.abs(mesh.nodes[ax] - v) <= tol)[0].astype(np.int64) + 1
+
+
+def dof(node, comp):
+    """dof (Mesh.jl:111): 3(node-1) + comp, both 1-based."""
+    return 3 * (np.asarray(node) - 1) + np.asarray(comp)
+
+
+# ------------------------------------------------------------------ material
+@dataclass
+class J2Material:
+    """J2Material (Materials.jl:68-108), linear isotropic hardening (Hkin = 0 on this path)."""
+    E: float
+    nu: float
+    sigy0: float
+    Hiso: float = 0.0
+    Hkin: float = 0.0
+
+    def __post_init__(self):
+        # ArgumentError guards, Materials.jl:90-103
+        if not self.E > 0:
+            raise ValueError(f"E must be positive (got {self.E})")
+        if not (-1 < self.nu < 0.5):
+            raise ValueError(f"nu must satisfy -1 < nu < 0.5 (got {self.nu})")
+        if not self.sigy0 > 0:
+            raise ValueError(f"sigy0 must be positive (got {self.sigy0})")
+        if self.Hiso < 0 or self.Hkin < 0:
+            raise ValueError("hardening moduli must be >= 0")
+
+    @property
+    def G(self):
+        return self.E / (2 * (1 + self.nu))
+
+    @property
+    def lam(self):
+        return self.E * self.nu / ((1 + self.nu) * (1 - 2 * self.nu))
+
+    def _c(self) -> L.Material:
+        return L.Material(self.E, self.nu, self.sigy0, self.Hiso, self.Hkin)
+
+
+@dataclass
+class SolveResult:
+    """SolveResult (Solver.jl:61-66) plus device timings."""
+    converged: bool
+    iters: list
+    residuals: list
+    cg_iters: list
+    stats: dict = field(default_factory=dict)
+
+
+_KINDS = {"finite": L.PFEM_HEX8_FINITE, "finite_fbar": L.PFEM_HEX8_FINITE_FBAR}
+_PREC = {"fp64": L.PFEM_FP64, "mixed": L.PFEM_MIXED}
+_PRED = {"previous": L.PFEM_PRED_PREVIOUS, "extrapolate": L.PFEM_PRED_EXTRAPOLATE,
+         "learned": L.PFEM_PRED_LEARNED}
+_KRY = {"cg": L.PFEM_KRYLOV_CG, "bicgstab": L.PFEM_KRYLOV_BICGSTAB}
+
+
+class Model:
+    """Model(mesh, material; element=:finite_fbar) (Model.jl:63-75), on one GPU.
+
+    ``sigy0_e`` optionally gives a per-element initial yield stress.
+    """
+
+    def __init__(self, mesh: Mesh, material: J2Material, element: str = "finite_fbar",
+                 sigy0_e=None, device: int = 0):
+        element = element.lstrip(":")
+        if element not in _KINDS:
+            raise ValueError(f"unknown element kind {element} (use finite, finite_fbar)")
+        self.mesh = mesh
+        self.material = material
+        self.element = element
+        self.nn, self.ne = mesh.nnodes, mesh.nelem
+        self.ndof, self.ngp = 3 * self.nn, 8 * self.ne
+        nodes = np.ascontiguousarray(mesh.nodes.T, dtype=np.float64)        # (nn,3) = 3 x nn col-major
+        els = np.ascontiguousarray(mesh.elements.T, dtype=np.int64)          # (ne,8) = 8 x ne col-major
+        sy = None if sigy0_e is None else np.ascontiguousarray(sigy0_e, dtype=np.float64)
+        self._ctx = C.c_void_p()
+        m = material._c()
+        rc = L.lib().pfem_create(C.byref(self._ctx), ptr(nodes), self.nn, ptr(els, L._i64), self.ne,
+                                 _KINDS[element], C.byref(m), ptr(sy), device)
+        check(rc, None)
+        self.dir_dofs, self.dir_vals, self.dir_ramp = [], [], []
+        self.neu_dofs, self.neu_vals = [], []
+        self._bcs_dirty = True
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx is not None and ctx.value:
+            try:
+                L.lib().pfem_destroy(ctx)
+            except Exception:
+                pass
+            self._ctx = None
+
+    # --- BC builders (Model.jl:102-145) ---
+    @staticmethod
+    def _comps(comp):
+        comp = comp.lstrip(":")
+        return {"x": (1,), "y": (2,), "z": (3,), "all": (1, 2, 3)}[comp]
+
+    def fix(self, nodes, comp="all"):
+        for n in np.atleast_1d(nodes):
+            for c in self._comps(comp):
+                self.dir_dofs.append(3 * (int(n) - 1) + c); self.dir_vals.append(0.0); self.dir_ramp.append(0)
+        self._bcs_dirty = True
+        return self
+
+    def prescribe(self, nodes, comp, value, ramp=True):
+        for n in np.atleast_1d(nodes):
+            for c in self._comps(comp):
+                self.dir_dofs.append(3 * (int(n) - 1) + c); self.dir_vals.append(float(value))
+                self.dir_ramp.append(1 if ramp else 0)
+        self._bcs_dirty = True
+        return self
+
+    def load(self, nodes, comp, value, distribute=False):
+        nodes = np.atleast_1d(nodes)
+        per = float(value) / len(nodes) if distribute else float(value)
+        for n in nodes:
+            for c in self._comps(comp):
+                self.neu_dofs.append(3 * (int(n) - 1) + c); self.neu_vals.append(per)
+        self._bcs_dirty = True
+        return self
+
+    def _push_bcs(self):
+        if not self._bcs_dirty:
+            return
+        dd = np.asarray(self.dir_dofs, np.int64); dv = np.asarray(self.dir_vals, np.float64)
+        dr = np.asarray(self.dir_ramp, np.uint8)
+        nd = np.asarray(self.neu_dofs, np.int64); nv = np.asarray(self.neu_vals, np.float64)
+        rc = L.lib().pfem_set_bcs(self._ctx, ptr(dd, L._i64), ptr(dv), ptr(dr, L._u8), len(dd),
+                                  ptr(nd, L._i64), ptr(nv), len(nd))
+        check(rc, self._ctx)
+        self._bcs_dirty = False
+
+    # --- structure ---
+    def pattern(self):
+        """1-based CSC colptr/rowval (int64) of SparsityPattern.K (Assembly.jl:99-148)."""
+        nnz = C.c_int64()
+        check(L.lib().pfem_pattern(self._ctx, C.byref(nnz), None, None), self._ctx)
+        colptr = np.zeros(self.ndof + 1, np.int64)
+        rowval = np.zeros(nnz.value, np.int64)
+        check(L.lib().pfem_pattern(self._ctx, C.byref(nnz), ptr(colptr, L._i64), ptr(rowval, L._i64)),
+              self._ctx)
+        return colptr, rowval
+
+    def colors(self):
+        nc = C.c_int32()
+        col = np.zeros(self.ne, np.int64)
+        check(L.lib().pfem_colors(self._ctx, C.byref(nc), ptr(col, L._i64)), self._ctx)
+        return nc.value, col
+
+    # --- hot path ---
+    def assemble(self, U, commit=False, precision="fp64", want_K=True):
+        """assemble! (Assembly.jl:238-257) -> (K scipy.csr or None, R, tau (ngp,6), flags)."""
+        U = np.ascontiguousarray(U, np.float64)
+        R = np.zeros(self.ndof)
+        tau = np.zeros((self.ngp, 6))
+        fl = np.zeros(self.ngp, np.uint8)
+        K = None
+        if want_K and not commit:
+            colptr, rowval = self.pattern()
+            kv = np.zeros(len(rowval))
+            rc = L.lib().pfem_assemble(self._ctx, ptr(U), int(commit), _PREC[precision], ptr(R), ptr(kv),
+                                       ptr(tau), ptr(fl, L._u8))
+            check(rc, self._ctx)
+            K = sp.csr_matrix((kv, rowval - 1, colptr - 1), shape=(self.ndof, self.ndof))
+        else:
+            rc = L.lib().pfem_assemble(self._ctx, ptr(U), int(commit), _PREC[precision], ptr(R), None,
+                                       ptr(tau), ptr(fl, L._u8))
+            check(rc, self._ctx)
+        return K, R, tau, fl
+
+    def _opts(self, nsteps=10, tol=1e-8, maxiter=25, precision="fp64", linsolve="cg", lin_rtol=None,
+              predictor="previous", amg_rebuild=False, cheb_degree=2, cg_itmax=200, eta_min=None,
+              line_search=False, verbose=False):
+        o = L.SolveOpts()
+        L.lib().pfem_default_opts(C.byref(o))
+        o.nsteps, o.maxiter, o.tol = nsteps, maxiter, tol
+        o.precision = _PREC[precision]
+        o.krylov = _KRY[linsolve]
+        o.lin_rtol = -1.0 if lin_rtol is None else float(lin_rtol)
+        if eta_min is not None:
+            o.eta_min = eta_min
+        elif precision == "mixed":
+            o.eta_min = 1e-6   # FP32 inner solves cannot go much below this
+        o.predictor = _PRED[predictor]
+        o.amg_rebuild = int(bool(amg_rebuild))
+        o.cheb_degree = cheb_degree
+        o.krylov_itmax = cg_itmax
+        o.verbose = int(bool(verbose))
+        o.line_search = int(bool(line_search))
+        return o
+
+    def solve(self, nsteps=10, tol=1e-8, maxiter=25, **kw) -> SolveResult:
+        """solve! (Solver.jl:419-475) on the GPU."""
+        self._push_bcs()
+        o = self._opts(nsteps=nsteps, tol=tol, maxiter=maxiter, **kw)
+        res = L.SolveResultC()
+        its = np.zeros(nsteps, np.int32)
+        hist = np.zeros((nsteps, maxiter))
+        kh = np.zeros((nsteps, maxiter), np.int32)
+        rc = L.lib().pfem_solve(self._ctx, C.byref(o), C.byref(res), ptr(its, L._i32), ptr(hist),
+                                ptr(kh, L._i32))
+        if rc not in (L.PFEM_OK, L.PFEM_ERR_NOT_CONVERGED):
+            check(rc, self._ctx)
+        n = max(res.steps_done + (0 if res.converged else 1), 0)
+        iters = [int(i) for i in its[:n]]
+        residuals = [list(hist[s, :iters[s]]) for s in range(n)]
+        cg = [list(map(int, kh[s, :max(iters[s] - 1, 0)])) for s in range(n)]
+        stats = {k: getattr(res, k) for k, _ in L.SolveResultC._fields_}
+        return SolveResult(bool(res.converged), iters, residuals, cg, stats)
+
+    def newton(self, lam, **kw):
+        """newton! (Solver.jl:317-389) for one load step + commit."""
+        self._push_bcs()
+        o = self._opts(**kw)
+        it = C.c_int32()
+        hist = np.zeros(o.maxiter)
+        kh = np.zeros(o.maxiter, np.int32)
+        rc = L.lib().pfem_newton(self._ctx, float(lam), C.byref(o), C.byref(it), ptr(hist), ptr(kh, L._i32))
+        check(rc, self._ctx)
+        return list(hist[:it.value]), list(kh[:max(it.value - 1, 0)])
+
+    def linear_solve(self, b, rtol, rebuild=True, **kw):
+        o = self._opts(**kw)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.ndof)
+        n = C.c_int32()
+        rc = L.lib().pfem_linear_solve(self._ctx, ptr(b), ptr(x), float(rtol), int(rebuild), C.byref(o),
+                                       C.byref(n))
+        check(rc, self._ctx)
+        return x, n.value
+
+    def reset(self):
+        check(L.lib().pfem_reset(self._ctx), self._ctx)
+        return self
+
+    def set_state(self, cpi=None, alpha=None, epsp=None):
+        """Overwrite the committed per-GP state (arrays shaped (ngp, 6) / (ngp,))."""
+        c = None if cpi is None else np.ascontiguousarray(cpi, np.float64)
+        a = None if alpha is None else np.ascontiguousarray(alpha, np.float64)
+        e = None if epsp is None else np.ascontiguousarray(epsp, np.float64)
+        check(L.lib().pfem_set_state(self._ctx, ptr(c), ptr(a), ptr(e)), self._ctx)
+
+    def set_displacement(self, U):
+        U = np.ascontiguousarray(U, np.float64)
+        check(L.lib().pfem_set_displacement(self._ctx, ptr(U)), self._ctx)
+
+    def state(self):
+        U = np.zeros(self.ndof)
+        tau = np.zeros((self.ngp, 6)); cpi = np.zeros((self.ngp, 6)); ep = np.zeros((self.ngp, 6))
+        al = np.zeros(self.ngp); fl = np.zeros(self.ngp, np.uint8)
+        rc = L.lib().pfem_get_state(self._ctx, ptr(U), ptr(tau), ptr(al), ptr(cpi), ptr(ep), ptr(fl, L._u8))
+        check(rc, self._ctx)
+        return dict(U=U, tau=tau, alpha=al, cpi=cpi, epsp=ep, flags=fl)
+
+    @property
+    def U(self):
+        U = np.zeros(self.ndof)
+        check(L.lib().pfem_get_state(self._ctx, ptr(U), None, None, None, None, None), self._ctx)
+        return U
+
+    def profile(self, what: int, reps: int = 10) -> float:
+        ms = C.c_double()
+        check(L.lib().pfem_profile(self._ctx, what, reps, C.byref(ms)), self._ctx)
+        return ms.value
+
+
+# ------------------------------------------------------------------ free functions
+def fix(model, nodes, comp="all"):
+    return model.fix(nodes, comp)
+
+
+def prescribe(model, nodes, comp, value, ramp=True):
+    return model.prescribe(nodes, comp, value, ramp)
+
+
+def load(model, nodes, comp, value, distribute=False):
+    return model.load(nodes, comp, value, distribute)
+
+
+def solve(model, **kw) -> SolveResult:
+    return model.solve(**kw)
+
+
+def reset(model):
+    return model.reset()
+
+
+def nodal_displacements(model) -> np.ndarray:
+    """nodal_displacements (Model.jl:169-178): 3 x nn."""
+    return model.U.reshape(-1, 3).T.copy()
+
+
+def gauss_kirchhoff(model) -> np.ndarray:
+    """Committed Kirchhoff stress, 6 x ngp (Model.jl:227)."""
+    return model.state()["tau"].T.copy()
+
+
+def gauss_stress(model) -> np.ndarray:
+    """Cauchy stress tau / det F (standard F), 6 x ngp (Model.jl:188-208)."""
+    s = np.zeros((model.ngp, 6))
+    check(L.lib().pfem_gauss_stress(model._ctx, ptr(s)), model._ctx)
+    return s.T.copy()
+
+
+def equivalent_plastic_strain(model) -> np.ndarray:
+    """Committed equivalent plastic strain alpha per GP (Model.jl:232)."""
+    return model.state()["alpha"]

@@ -1,0 +1,62 @@
+"""Generate the golden fixtures under tests/golden/ from the CPU oracle.
+
+The reference (Julia) cannot run on these machines, so the oracle -- pinned by
+tests/test_oracle_pins.py against the reference's own known-answer and
+finite-difference tests -- produces these vectors.  Run:
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle as O  # noqa: E402
+from plasticity_b200 import workloads as W  # noqa: E402
+
+
+def element_cases():
+    mat = O.J2Material(200e3, 0.3, 250.0, 2000.0)
+    nodes, el = O.box_mesh(1, 1, 1, 1, 1, 1)
+    Xu = nodes.T[el[:, 0] - 1]
+    S = np.array([[1.0, 0.15, 0.05], [0.0, 1.0, 0.1], [0.0, 0.0, 1.0]])
+    Xd = Xu @ S.T + 0.03 * np.sin(np.arange(24)).reshape(8, 3)     # distorted element
+    Fs = [np.eye(3),
+          np.diag([1.001, 0.9995, 1.0003]),
+          np.array([[1.05, 0.025, 0.005], [0.04, 0.98, 0.01], [0.01, 0.015, 1.02]]),
+          np.array([[1.1, 0.05, 0.01], [0.08, 0.96, 0.02], [0.02, 0.03, 1.04]]),
+          np.array([[0.85, 0.02, 0.0], [0.01, 1.07, 0.03], [0.0, 0.02, 1.06]])]
+    out = {k: [] for k in ["fbar", "Xe", "ue", "cpi", "alpha", "Fe", "Ke", "tau", "flags", "cpi_new", "alpha_new"]}
+    for fbar in (0, 1):
+        for Xe in (Xu, Xd):
+            cpi = np.tile([1, 1, 1, 0, 0, 0.0], (8, 1)); alpha = np.zeros(8)
+            for F in Fs:
+                ue = np.array([F @ x - x for x in Xe]).reshape(24)
+                ue = ue + 1e-3 * np.cos(np.arange(24))           # non-homogeneous part
+                r = O.element(fbar, mat, Xe, ue, cpi, alpha)
+                for k, v in [("fbar", fbar), ("Xe", Xe), ("ue", ue), ("cpi", cpi), ("alpha", alpha),
+                             ("Fe", r["Fe"]), ("Ke", r["Ke"]), ("tau", r["tau"]), ("flags", r["flags"]),
+                             ("cpi_new", r["cpi_new"]), ("alpha_new", r["alpha"])]:
+                    out[k].append(np.array(v))
+                cpi, alpha = r["cpi_new"], r["alpha"]          # commit: path-dependent chain
+    np.savez_compressed(os.path.join(HERE, "element_cases.npz"), **{k: np.array(v) for k, v in out.items()})
+
+
+def solve_case(w, fname, line_search=False):
+    mat = O.J2Material(**{k: w.material[k] for k in ("E", "nu", "sigy0", "Hiso", "Hkin")})
+    m = O.OracleModel(w.mesh.nodes, w.mesh.elements, mat, fbar=True, sigy0_e=w.sigy0_e)
+    w.apply(m)
+    res = m.solve(nsteps=w.nsteps, tol=w.tol, maxiter=25, line_search=line_search)
+    assert res["converged"]
+    np.savez_compressed(os.path.join(HERE, fname), U=m.U, tau=m.tau, alpha=m.alpha, flags=m.flags,
+                        sigma=m.gauss_stress(), iters=np.array(res["iters"]), nsteps=w.nsteps, tol=w.tol, line_search=int(line_search))
+    print(fname, res["iters"], float(np.abs(m.U).max()), float(m.alpha.max()), float(m.flags.mean()))
+
+
+if __name__ == "__main__":
+    element_cases()
+    solve_case(W.config0(n=8), "config0_cube8.npz")
+    solve_case(W.config2(n=4, nsteps=40), "cube4_jitter_compress.npz", line_search=True)
+    solve_case(W.config1(nx=8, ny=2, nz=2, nsteps=6, stretch=0.05), "bar8x2x2_neck.npz")

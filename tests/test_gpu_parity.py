@@ -1,0 +1,190 @@
+"""GPU parity of the CUDA path against the CPU oracle and its golden fixtures.
+
+Bars (north_star): CSR pattern, colors and per-Gauss-point elastic/plastic flags
+bit-exact; converged displacements within 1e-8 relative; Cauchy stress and
+equivalent plastic strain within 1e-6 relative; Newton iterations within +-1.
+Element-level quantities use tighter FP64 bars (1e-9 normwise) and 1e-6 for the
+FP32 tangent.
+"""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import plasticity_b200 as P
+from plasticity_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(a, b):
+    a = np.asarray(a, float); b = np.asarray(b, float)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def model_from(w, **kw):
+    mat = P.J2Material(**w.material)
+    M = P.Model(w.mesh, mat, element="finite_fbar", sigy0_e=w.sigy0_e, **kw)
+    w.apply(M)
+    return M
+
+
+def one_element_model(Xe, fbar, mat):
+    mesh = P.Mesh(np.ascontiguousarray(np.asarray(Xe).T), np.arange(1, 9, dtype=np.int64).reshape(8, 1))
+    return P.Model(mesh, mat, element="finite_fbar" if fbar else "finite")
+
+
+def test_element_cases_vs_golden():
+    g = np.load(os.path.join(GOLD, "element_cases.npz"))
+    mat = P.J2Material(200e3, 0.3, 250.0, 2000.0)
+    for i in range(len(g["fbar"])):
+        M = one_element_model(g["Xe"][i], int(g["fbar"][i]), mat)
+        M.set_state(cpi=g["cpi"][i], alpha=g["alpha"][i])
+        K, R, tau, fl = M.assemble(g["ue"][i])
+        assert rel(R, g["Fe"][i]) < 1e-10, i
+        assert rel(K.toarray(), g["Ke"][i]) < 1e-9, i
+        assert rel(tau, g["tau"][i]) < 1e-10, i
+        assert np.array_equal(fl, g["flags"][i]), i
+        K32, R32, _, _ = M.assemble(g["ue"][i], precision="mixed")
+        assert rel(K32.toarray(), g["Ke"][i]) < 1e-6, i
+        assert rel(R32, g["Fe"][i]) < 1e-10, i
+        M.assemble(g["ue"][i], commit=True)
+        st = M.state()
+        assert rel(st["cpi"], g["cpi_new"][i]) < 1e-12, i
+        assert np.abs(st["alpha"] - g["alpha_new"][i]).max() < 1e-12, i
+
+
+@pytest.mark.parametrize("fbar", [True, False])
+def test_assembly_vs_oracle_jittered(oracle, fbar):
+    w = W.config2(n=5)
+    mat = P.J2Material(**w.material)
+    M = P.Model(w.mesh, mat, element="finite_fbar" if fbar else "finite", sigy0_e=w.sigy0_e)
+    om = oracle.OracleModel(w.mesh.nodes, w.mesh.elements, oracle.J2Material(**w.material), fbar=fbar,
+                            sigy0_e=w.sigy0_e)
+    rng = np.random.default_rng(7)
+    X = w.mesh.nodes
+    U = (np.stack([0.004 * X[0], 0.002 * X[1], -0.008 * X[2]]).T.reshape(-1)
+         + 2e-4 * rng.standard_normal(M.ndof))
+    # a plastic committed state from one commit at a smaller load
+    M.assemble(0.5 * U, commit=True)
+    om.assemble(0.5 * U, commit=True)
+    K, R, tau, fl = M.assemble(U)
+    Ko, Ro, tauo, flo = om.assemble(U)
+    assert rel(R, Ro) < 1e-10
+    assert abs(K - Ko.tocsr()).max() / abs(Ko).max() < 1e-10
+    assert rel(tau, tauo) < 1e-10
+    assert np.array_equal(fl, flo) and fl.mean() > 0.5
+    K32, _, _, _ = M.assemble(U, precision="mixed")
+    assert abs(K32 - Ko.tocsr()).max() / abs(Ko).max() < 1e-6
+    cp, rv = M.pattern()
+    assert np.array_equal(cp, om.colptr) and np.array_equal(rv, om.rowval)
+
+
+def _check_solve(M, g, prec_label, iters_tol=1):
+    st = M.state()
+    U = st["U"]
+    assert rel(U, g["U"]) < 1e-8, prec_label
+    sig = P.gauss_stress(M).T
+    assert np.abs(sig - g["sigma"]).max() / np.abs(g["sigma"]).max() < 1e-6, prec_label
+    a = st["alpha"]
+    assert np.abs(a - g["alpha"]).max() / max(np.abs(g["alpha"]).max(), 1e-300) < 1e-6, prec_label
+    assert np.array_equal(st["flags"], g["flags"]), prec_label
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config0_solve_vs_golden(precision):
+    g = np.load(os.path.join(GOLD, "config0_cube8.npz"))
+    w = W.config0(n=8)
+    M = model_from(w)
+    res = M.solve(nsteps=int(g["nsteps"]), tol=float(g["tol"]), maxiter=25, precision=precision,
+                  lin_rtol=1e-12 if precision == "fp64" else 1e-6)
+    assert res.converged
+    _check_solve(M, g, precision)
+    d = np.abs(np.array(res.iters) - g["iters"])
+    assert d.max() <= 1, (res.iters, list(g["iters"]))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_jittered_compression_vs_golden(precision):
+    g = np.load(os.path.join(GOLD, "cube4_jitter_compress.npz"))
+    w = W.config2(n=4, nsteps=int(g["nsteps"]))
+    M = model_from(w)
+    res = M.solve(nsteps=w.nsteps, tol=w.tol, maxiter=25, precision=precision, line_search=True,
+                  lin_rtol=1e-12 if precision == "fp64" else None)
+    assert res.converged
+    _check_solve(M, g, precision)
+    if precision == "fp64":
+        assert np.abs(np.array(res.iters) - g["iters"]).max() <= 1
+
+
+def test_necking_bar_vs_golden():
+    g = np.load(os.path.join(GOLD, "bar8x2x2_neck.npz"))
+    w = W.config1(nx=8, ny=2, nz=2, nsteps=6, stretch=0.05)
+    M = model_from(w)
+    res = M.solve(nsteps=w.nsteps, tol=w.tol, maxiter=25, lin_rtol=1e-12)
+    assert res.converged
+    _check_solve(M, g, "fp64")
+    assert np.abs(np.array(res.iters) - g["iters"]).max() <= 1
+
+
+def test_predictors_reach_same_solution():
+    w = W.config0(n=6, nsteps=6)
+    sols = {}
+    for pred in ("previous", "extrapolate"):
+        M = model_from(w)
+        res = M.solve(nsteps=w.nsteps, tol=1e-10, predictor=pred, lin_rtol=1e-12)
+        assert res.converged
+        sols[pred] = (M.U, sum(res.iters))
+    assert rel(sols["extrapolate"][0], sols["previous"][0]) < 1e-8
+    assert sols["extrapolate"][1] <= sols["previous"][1]
+
+
+def test_bicgstab_matches_cg():
+    w = W.config0(n=6, nsteps=3)
+    out = []
+    for kry in ("cg", "bicgstab"):
+        M = model_from(w)
+        res = M.solve(nsteps=3, tol=1e-10, linsolve=kry, lin_rtol=1e-12)
+        assert res.converged
+        out.append(M.U)
+    assert rel(out[1], out[0]) < 1e-8
+
+
+def test_linear_solve_vs_direct(oracle):
+    w = W.config0(n=6, nsteps=4)
+    M = model_from(w)
+    M.newton(0.25, maxiter=25, tol=1e-10, lin_rtol=1e-12)
+    U = M.U
+    # the oracle's imposed tangent at the same displacement / committed state
+    om = oracle.OracleModel(w.mesh.nodes, w.mesh.elements, oracle.J2Material(**w.material), fbar=True)
+    w.apply(om)
+    ramp, fix = om.freeze_bcs()   # oracle state is the pre-step (virgin) committed state
+    Ko, Ro, _, _ = om.assemble(U)
+    om.impose(Ko, Ro, ramp[0], ramp[1], True, 0.25, U)
+    om.impose(Ko, Ro, fix[0], fix[1], False, 0.25, U)
+    b = np.sin(np.arange(M.ndof) * 0.37)
+    x_ref = spla.splu(Ko.tocsc()).solve(b)
+    x, it = M.linear_solve(b, rtol=1e-10)
+    assert rel(x, x_ref) < 1e-7 and it < 100
+
+
+def test_inverted_element_fails_loudly():
+    mat = P.J2Material(200e3, 0.3, 250.0, 2000.0)
+    Xe = P.box_mesh(1, 1, 1, 1, 1, 1).nodes.T
+    for fbar in (0, 1):
+        M = one_element_model(Xe, fbar, mat)
+        F = np.diag([-1.1, 1.0, 1.0])
+        ue = np.array([F @ x - x for x in Xe]).reshape(24)
+        with pytest.raises(P.PfemError) as e:
+            M.assemble(ue)
+        assert e.value.code == -3 and "inverted" in str(e.value)
+
+
+def test_profile_reports_kernel_times():
+    w = W.config0(n=8)
+    M = model_from(w)
+    for what in (0, 1, 2, 3):
+        assert M.profile(what, reps=3) > 0

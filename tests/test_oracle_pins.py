@@ -1,0 +1,280 @@
+"""Pin the CPU oracle against the reference's own known-answer and FD tests.
+
+Each test restates one from vinaysrao1/plasticity lagrangian/test/*.jl on the
+oracle (the checker of the GPU path).  The F2 finite-difference gates use the
+reference's deformation gradients with Hkin = 0 (this path's material class).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+E, NU, SY, HI = 210e3, 0.3, 250.0, 1000.0
+
+
+def _uniaxial(O, mat, exx_t, nsteps=50):
+    ep = np.zeros(6); b = np.zeros(6); a = 0.0; el = 0.0
+    for n in range(1, nsteps + 1):
+        exx = exx_t * n / nsteps
+        for _ in range(60):
+            s, _, _, _, D, _ = O.return_map(mat, [exx, el, el, 0, 0, 0], ep, b, a)
+            el -= s[1] / (D[1, 1] + D[1, 2])
+            if abs(s[1]) < 1e-11:
+                break
+        s, ep, b, a, _, _ = O.return_map(mat, [exx, el, el, 0, 0, 0], ep, b, a)
+    return O.return_map(mat, [exx_t, el, el, 0, 0, 0], ep, b, a)[0]
+
+
+def test_T1_elastic_roundtrip(oracle):
+    # test_material.jl:11-21
+    mat = oracle.J2Material(E, NU, SY, HI, 500.0)
+    eps = np.array([1e-4, -2e-5, 3e-5, 1e-5, -1e-5, 2e-5])
+    s, ep, b, a, D, pl = oracle.return_map(mat, eps)
+    np.testing.assert_allclose(s, mat.cmat() @ eps, rtol=1e-12)
+    assert pl == 0 and a == 0.0 and not ep.any()
+    np.testing.assert_allclose(D, mat.cmat(), rtol=1e-12)
+
+
+@pytest.mark.parametrize("exx", [0.004, 0.007, 0.01])
+def test_T2_uniaxial_closed_form(oracle, exx):
+    # test_material.jl:23-52; 258.77 MPa at exx = 0.01 (docs/DESIGN.md T2)
+    mat = oracle.J2Material(E, NU, SY, HI)
+    s = _uniaxial(oracle, mat, exx)
+    Ht = E * HI / (E + HI)
+    assert s[0] == pytest.approx(SY + Ht * (exx - SY / E), rel=1e-6)
+    assert abs(s[1]) < 1e-6 * s[0]
+    if exx == 0.01:
+        assert s[0] == pytest.approx(258.77, abs=5e-3)
+
+
+def test_T3_perfect_plasticity_cap(oracle):
+    # test_material.jl:54-76
+    mat = oracle.J2Material(E, NU, SY, 0.0)
+    ep = np.zeros(6); b = np.zeros(6); a = 0.0; el = 0.0; sxx = 0.0
+    for n in range(1, 201):
+        exx = 0.02 * n / 200
+        for _ in range(60):
+            s, _, _, _, D, _ = oracle.return_map(mat, [exx, el, el, 0, 0, 0], ep, b, a)
+            d = D[1, 1] + D[1, 2]
+            if d == 0:
+                break
+            el -= s[1] / d
+            if abs(s[1]) < 1e-9:
+                break
+        s, ep, b, a, _, _ = oracle.return_map(mat, [exx, el, el, 0, 0, 0], ep, b, a)
+        sxx = s[0]
+        assert sxx <= SY * (1 + 1e-10)
+    assert sxx == pytest.approx(SY, rel=1e-3)
+
+
+@pytest.mark.parametrize("eps", [[0.01, 0, 0, 0, 0, 0], [0.005, -0.001, 0, 0.004, 0.002, 0],
+                                 [0.003, -0.002, 0.001, 0.002, 0.001, 0.0015], [0, 0, 0, 0.006, 0, 0]])
+def test_T5_T6_consistent_tangent(oracle, eps):
+    # test_material.jl:128-157 (Hkin = 0 here)
+    mat = oracle.J2Material(E, NU, SY, HI)
+    eps = np.array(eps, float)
+    D = oracle.return_map(mat, eps)[4]
+    h = 1e-7
+    Dfd = np.zeros((6, 6))
+    for j in range(6):
+        e = np.zeros(6); e[j] = h
+        Dfd[:, j] = (oracle.return_map(mat, eps + e)[0] - oracle.return_map(mat, eps - e)[0]) / (2 * h)
+    assert np.linalg.norm(D - Dfd) / np.linalg.norm(D) <= 1e-5
+    assert np.linalg.norm(D - D.T) <= 1e-12 * np.linalg.norm(D)
+
+
+def test_T7_plastic_incompressibility(oracle):
+    mat = oracle.J2Material(E, NU, SY, HI)
+    eps = np.array([0.01, -0.002, 0.001, 0.003, 0, 0])
+    s, ep, _, _, _, _ = oracle.return_map(mat, eps)
+    assert abs(ep[:3].sum()) < 1e-12
+    st = mat.cmat() @ eps
+    assert s[:3].mean() == pytest.approx(st[:3].mean(), abs=1e-9)
+
+
+def _unit(O):
+    nodes, el = O.box_mesh(1, 1, 1, 1, 1, 1)
+    return nodes.T[el[:, 0] - 1]
+
+
+def _ue(Xe, F):
+    return np.array([F @ x - x for x in Xe]).reshape(24)
+
+
+def _fd(O, fbar, mat, Xe, ue, cpi=None, alpha=None, h=1e-7):
+    r = O.element(fbar, mat, Xe, ue, cpi, alpha)
+    K = r["Ke"]
+    Kfd = np.zeros((24, 24))
+    for j in range(24):
+        up = ue.copy(); up[j] += h
+        um = ue.copy(); um[j] -= h
+        Kfd[:, j] = (O.element(fbar, mat, Xe, up, cpi, alpha)["Fe"] -
+                     O.element(fbar, mat, Xe, um, cpi, alpha)["Fe"]) / (2 * h)
+    return np.linalg.norm(Kfd - K) / np.linalg.norm(K), np.linalg.norm(K - K.T) / np.linalg.norm(K)
+
+
+F1 = np.array([[1.05, 0.025, 0.005], [0.04, 0.98, 0.01], [0.01, 0.015, 1.02]])
+F2 = np.array([[1.1, 0.05, 0.01], [0.08, 0.96, 0.02], [0.02, 0.03, 1.04]])
+
+
+@pytest.mark.parametrize("F", [np.diag([1.1, 0.95, 1.03]),
+                               np.array([[1.08, 0.03, 0.01], [0.04, 0.97, 0.0], [0.0, 0.02, 1.05]])])
+def test_F2a_elastic_fd_tangent(oracle, F):
+    # test_finite_strain.jl:119-126
+    mat = oracle.J2Material(E, NU, SY, HI)
+    rel, _ = _fd(oracle, 0, mat, _unit(oracle), _ue(_unit(oracle), F))
+    assert rel < 1e-6
+
+
+def test_F2b_plastic_path_fd_tangent(oracle):
+    # test_finite_strain.jl:128-138: incremental plastic loading, committed history
+    mat = oracle.J2Material(E, NU, SY, HI)
+    Xe = _unit(oracle)
+    cpi = None; alpha = None
+    for k in range(1, 9):
+        Fk = np.diag([1 + 0.02 * k, 1 - 0.008 * k, 1 - 0.008 * k])
+        rel, _ = _fd(oracle, 0, mat, Xe, _ue(Xe, Fk), cpi, alpha)
+        assert rel < 1e-6
+        r = oracle.element(0, mat, Xe, _ue(Xe, Fk), cpi, alpha)
+        cpi, alpha = r["cpi_new"], r["alpha"]
+    assert alpha.max() > 0.05
+
+
+@pytest.mark.parametrize("fbar", [0, 1])
+def test_F2cd_noncoaxial_and_fbar_fd_tangent(oracle, fbar):
+    # test_finite_strain.jl:140-155 (c) standard and (d) F-bar
+    mat = oracle.J2Material(E, NU, SY, HI)
+    Xe = _unit(oracle)
+    rel, _ = _fd(oracle, fbar, mat, Xe, _ue(Xe, F2))
+    assert rel < 1e-6
+    r = oracle.element(fbar, mat, Xe, _ue(Xe, F1))
+    rel, sym = _fd(oracle, fbar, mat, Xe, _ue(Xe, F2), r["cpi_new"], r["alpha"])
+    assert rel < 1e-6
+    if fbar:
+        assert sym > 1e-6          # F-bar tangent is genuinely non-symmetric
+    else:
+        assert sym < 1e-10         # F9: isotropic finite-strain tangent is symmetric
+
+
+@pytest.mark.parametrize("F", [np.array([[1.2, 0.03, 0], [0.05, 0.92, 0], [0, 0, 0.95]]),
+                               np.array([[1.3, 0.08, 0.02], [0.1, 0.9, 0.04], [0.05, 0.03, 0.85]])])
+def test_F3_det_Fp_is_one(oracle, F):
+    # test_finite_strain.jl:170-180
+    mat = oracle.J2Material(E, NU, SY, HI)
+    u = oracle.finite_update(mat, F)
+    assert u["alpha"] > 0
+    c = u["cpi_new"]
+    C = np.array([[c[0], c[3], c[5]], [c[3], c[1], c[4]], [c[5], c[4], c[2]]])
+    assert abs(1 / np.sqrt(np.linalg.det(C)) - 1) < 1e-12
+
+
+def test_F4_objectivity(oracle):
+    # test_finite_strain.jl:182-195
+    mat = oracle.J2Material(E, NU, SY, HI)
+    F = np.array([[1.2, 0.03, 0], [0.05, 0.92, 0], [0, 0, 0.95]])
+    th = 0.7
+    Q = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+
+    def sig(F):
+        t = oracle.finite_update(mat, F)["tau"]
+        return np.array([[t[0], t[3], t[5]], [t[3], t[1], t[4]], [t[5], t[4], t[2]]]) / np.linalg.det(F)
+
+    s1, s2 = sig(F), sig(Q @ F)
+    assert np.linalg.norm(s2 - Q @ s1 @ Q.T) / np.linalg.norm(s1) < 1e-12
+
+
+def test_F5_elastic_cyclic_shear(oracle):
+    # test_finite_strain.jl:225-240
+    mat = oracle.J2Material(E, NU, 1e9)
+    for g in np.concatenate([np.linspace(0, 0.3, 8), np.linspace(0.3, 0, 8)]):
+        F = np.array([[1, g, 0], [0, 1, 0], [0, 0, 1.0]])
+        tau = oracle.finite_update(mat, F)["tau"]
+    assert np.linalg.norm(tau) < 1e-6 * mat.E
+
+
+def test_F5b_plastic_cyclic_shear(oracle):
+    # test_finite_strain.jl:242-268
+    mat = oracle.J2Material(E, NU, SY, HI)
+    gs = np.concatenate([np.linspace(0, .05, 6)[1:], np.linspace(.05, 0, 6)[1:],
+                         np.linspace(0, -.05, 6)[1:], np.linspace(-.05, 0, 6)[1:]])
+    cpi = np.array([1, 1, 1, 0, 0, 0.0]); a = 0.0; ap = 0.0
+    for g in gs:
+        F = np.array([[1, g, 0], [0, 1, 0], [0, 0, 1.0]])
+        u = oracle.finite_update(mat, F, cpi, a)
+        cpi, a, tau = u["cpi_new"], u["alpha"], u["tau"]
+        assert a >= ap - 1e-12
+        ap = a
+    assert a > 0
+    p = tau[:3].mean()
+    s = tau - np.array([p, p, p, 0, 0, 0])
+    seq = np.sqrt(1.5 * (s[0] ** 2 + s[1] ** 2 + s[2] ** 2 + 2 * (s[3] ** 2 + s[4] ** 2 + s[5] ** 2)))
+    assert seq <= SY + HI * a + 1e-6 * E
+
+
+def test_F13_inverted_element_fails_loudly(oracle):
+    # test_finite_strain.jl:417-443
+    mat = oracle.J2Material(E, NU, SY, HI)
+    Xe = _unit(oracle)
+    ue = _ue(Xe, np.diag([-1.1, 1.0, 1.0]))
+    for fbar in (0, 1):
+        with pytest.raises(oracle.ElementInversionError) as ei:
+            oracle.element(fbar, mat, Xe, ue)
+        assert ei.value.J < 0
+
+
+def test_pattern_matches_canonical_sparse(oracle):
+    # test_assembly.jl:10-36: CSC pattern == sparse(I, J, V) canonical pattern
+    nodes, el = oracle.box_mesh(1, 1, 1, 2, 2, 2)
+    cp, rv = oracle.pattern(nodes.shape[1], el)
+    I, J = [], []
+    for e in range(el.shape[1]):
+        ed = [3 * (el[c // 3, e] - 1) + c % 3 for c in range(24)]
+        for c in range(24):
+            for r in range(24):
+                I.append(ed[r]); J.append(ed[c])
+    n = 3 * nodes.shape[1]
+    K = sp.csc_matrix((np.ones(len(I)), (I, J)), shape=(n, n))
+    K.sum_duplicates(); K.sort_indices()
+    assert np.array_equal(cp - 1, K.indptr) and np.array_equal(rv - 1, K.indices)
+    # nnz / N <= 81 and grows toward 81 (test_scaling.jl:116-127)
+    ratios = []
+    for m in (4, 8):
+        nd, e2 = oracle.box_mesh(1, 1, 1, m, m, m)
+        c2, r2 = oracle.pattern(nd.shape[1], e2)
+        ratios.append(len(r2) / (3 * nd.shape[1]))
+    assert all(r <= 81 for r in ratios) and ratios[1] > ratios[0]
+
+
+def test_B9_assembly_equals_independent_coo(oracle):
+    # hard_validation.jl:424-454 on the finite F-bar kernel at a deformed state
+    nodes, el = oracle.box_mesh(1, 1, 1, 2, 2, 2)
+    mat = oracle.J2Material(E, NU, SY, HI)
+    m = oracle.OracleModel(nodes, el, mat, fbar=True)
+    rng = np.random.default_rng(3)
+    U = 1e-3 * rng.standard_normal(m.ndof)
+    K, R, _, _ = m.assemble(U)
+    I, J, V = [], [], []
+    Rr = np.zeros(m.ndof)
+    for e in range(el.shape[1]):
+        ed = np.array([3 * (el[c // 3, e] - 1) + c % 3 for c in range(24)])
+        r = oracle.element(1, mat, nodes.T[el[:, e] - 1], U[ed])
+        for c in range(24):
+            for q in range(24):
+                I.append(ed[q]); J.append(ed[c]); V.append(r["Ke"][q, c])
+        Rr[ed] += r["Fe"]
+    Ki = sp.csc_matrix((V, (I, J)), shape=K.shape)
+    assert abs(K - Ki).max() <= 1e-12 * abs(K).max()
+    np.testing.assert_allclose(R, Rr, rtol=1e-12, atol=1e-9)
+
+
+def test_F11_fbar_newton_converges_quadratically(oracle):
+    # test_finite_strain.jl:343-374 (F-bar, nu = 0.49, rollers + x pull)
+    nodes, el = oracle.box_mesh(1, 1, 1, 3, 3, 3)
+    m = oracle.OracleModel(nodes, el, oracle.J2Material(E, 0.49, SY, HI), fbar=True)
+    face = lambda d, v: list(np.nonzero(np.abs(nodes[d] - v) <= 1e-8)[0] + 1)
+    m.fix(face(0, 0), "x"); m.fix(face(1, 0), "y"); m.fix(face(2, 0), "z")
+    m.prescribe(face(0, 1), "x", 0.08)
+    res = m.solve(nsteps=4, tol=1e-8)
+    assert res["converged"]
+    assert m.alpha.max() > 0.05
+    h = res["residuals"][-1]
+    assert any(h[k + 1] <= 50 * h[k] ** 2 + 1e-12 for k in range(1, len(h) - 1) if h[k] < 1)
