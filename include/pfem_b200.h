@@ -146,10 +146,26 @@ int pfem_newton(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, int32_t*
 int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res,
                int32_t* iters_per_step, double* residuals, int32_t* krylov_per_iter);
 
+/* One Newton iteration's assembly at the context's current U against the
+ * committed state: K and R (Assembly.jl:238-257), R -= lambda Fext, Dirichlet
+ * imposition of both BC sets (Solver.jl:349-355), ||R|| (Solver.jl:358).  The
+ * imposed tangent stays resident for pfem_linear_solve; R (ndof) is copied
+ * out when non-null. */
+int pfem_residual(pfem_ctx* ctx, double lambda, int32_t precision, double* rnorm, double* R);
+
 /* _linear_solve! (Solver.jl:235-290) on the tangent left by the last Newton
  * iteration (Dirichlet rows imposed): x = K^-1 b to relative tolerance rtol. */
 int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, int32_t rebuild_pc,
                       const pfem_solve_opts* o, int32_t* niter);
+
+/* One V-cycle of the AMG hierarchy last built by pfem_linear_solve / Newton
+ * (precision of the resident tangent): z = M^-1 r, host vectors of ndof. */
+int pfem_amg_apply(pfem_ctx* ctx, const double* r, double* z);
+
+/* Inspection of the resident AMG hierarchy (small problems): the dense
+ * operator of `level` (what = 0, n_l x n_l, row-major) or its smoothed
+ * prolongator (what = 1, n_l x n_{l+1}); dims receives (rows, cols). */
+int pfem_amg_dense(pfem_ctx* ctx, int32_t level, int32_t what, double* out, int64_t* dims);
 
 /* Read-out: nodal_displacements / gauss_kirchhoff / equivalent_plastic_strain /
  * Cp^-1 / eps_p / last elastic-plastic flags (Model.jl:169-232).  Null pointers
@@ -169,6 +185,13 @@ int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma);
  * what: 0 = element kernels of one full assembly (all colors, FP64 tangent),
  *       1 = same with the FP32 tangent, 2 = level-0 SpMV FP32, 3 = SpMV FP64. */
 int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms_per_launch);
+
+/* CUDA-event timer on the context's stream (the stream every kernel of this
+ * context is launched on): op 0 records the start event; op 1 records the
+ * stop event, synchronizes and returns the elapsed milliseconds in *ms. */
+int pfem_timer(pfem_ctx* ctx, int32_t op, double* ms);
+/* Number of CUDA kernels this library has launched in this process. */
+int64_t pfem_kernel_launches(void);
 
 #ifdef __cplusplus
 }

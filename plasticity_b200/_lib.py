@@ -75,12 +75,17 @@ SIGNATURES = {
     "pfem_assemble": (C.c_int, [_ctx, _d, C.c_int32, C.c_int32, _d, _d, _d, _u8]),
     "pfem_newton": (C.c_int, [_ctx, C.c_double, C.POINTER(SolveOpts), _i32, _d, _i32]),
     "pfem_solve": (C.c_int, [_ctx, C.POINTER(SolveOpts), C.POINTER(SolveResultC), _i32, _d, _i32]),
+    "pfem_residual": (C.c_int, [_ctx, C.c_double, C.c_int32, _d, _d]),
     "pfem_linear_solve": (C.c_int, [_ctx, _d, _d, C.c_double, C.c_int32, C.POINTER(SolveOpts), _i32]),
+    "pfem_amg_apply": (C.c_int, [_ctx, _d, _d]),
+    "pfem_amg_dense": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d, _i64]),
     "pfem_get_state": (C.c_int, [_ctx, _d, _d, _d, _d, _d, _u8]),
     "pfem_set_state": (C.c_int, [_ctx, _d, _d, _d]),
     "pfem_set_displacement": (C.c_int, [_ctx, _d]),
     "pfem_gauss_stress": (C.c_int, [_ctx, _d]),
     "pfem_profile": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d]),
+    "pfem_timer": (C.c_int, [_ctx, C.c_int32, _d]),
+    "pfem_kernel_launches": (C.c_int64, []),
 }
 
 _lib = None

@@ -3,6 +3,7 @@
 // solvers and the aggregation AMG they use.
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -17,6 +18,8 @@
 using namespace pfem;
 
 static thread_local std::string g_cuda_err;
+static long long g_launches = 0;
+long long& pfem::launch_counter() { return g_launches; }
 void pfem_set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
   char buf[512];
   snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what,
@@ -38,10 +41,14 @@ struct KrylovWork {
 
 struct HostLevel {
   int nbrow = 0, bs = 0;
-  std::vector<int> rowptr, col;
+  std::vector<int> rowptr, col;   // matrix pattern of this level
+  std::vector<int> grp, gcl;      // graph the aggregates are grown on
   int nagg = 0;
-  std::vector<int> agg, aptr, amem, f2c;
-  std::vector<double> T;  // nbrow*bs*6
+  std::vector<int> agg;
+  std::vector<double> T;          // nbrow*bs*6 tentative prolongator blocks
+  std::vector<int> p_rp, p_cl, p_row, pslot, pt_rp, pt_blk;  // smoothed P pattern
+  std::vector<int> ap_rp, ap_cl, ap_row;                      // A P pattern
+  std::vector<int> c_row;         // row of every block of the next level's pattern
 };
 
 }  // namespace
@@ -91,7 +98,7 @@ struct pfem_ctx {
   KrylovWork<float> kw32;
   KrylovWork<double> kw64;
   int tangent_prec = -1;  // precision of the last imposed tangent
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
   // learned predictor
   pfem::MlpState mlp;
   int steps_taken = 0;
@@ -284,45 +291,56 @@ void mgs_qr(int m, std::vector<double>& A, double R[36]) {
   }
 }
 
-// Host side of the AMG hierarchy: aggregates, tentative prolongators from the
-// six rigid-body modes (Solver.jl:117-129), coarse patterns, fine->coarse maps.
+// Sorted union of the column lists of a set of rows.
+void sorted_union(std::vector<int>& out) {
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+}
+
+// Host side of the smoothed-aggregation hierarchy (one-time, mesh-only):
+// aggregates, tentative prolongators from the six rigid-body modes
+// (Solver.jl:117-129), and the patterns of P = (I - w D^-1 A) T, of A P and
+// of the Galerkin operator P^T A P of every level.
 void build_amg_structure(pfem_ctx* c) {
   c->hl.clear();
-  HostLevel L0;
-  L0.nbrow = (int)c->nn;
-  L0.bs = 3;
-  L0.rowptr = c->browptr;
-  L0.col = c->bcol;
-  std::vector<double> B((size_t)c->nn * 3 * 6, 0.0);  // rows (node,comp) x 6
+  HostLevel cur;
+  cur.nbrow = (int)c->nn;
+  cur.bs = 3;
+  cur.rowptr = c->browptr;
+  cur.col = c->bcol;
+  cur.grp = c->browptr;
+  cur.gcl = c->bcol;
+  std::vector<double> B;
+  double ctr[3] = {0, 0, 0};
+  for (long long n = 0; n < c->nn; ++n)
+    for (int d = 0; d < 3; ++d) ctr[d] += c->X[n * 3 + d] / (double)c->nn;
   bool first = true;
-  HostLevel cur = std::move(L0);
   for (int lev = 0; lev < 10; ++lev) {
     const int nb = cur.nbrow, bs = cur.bs;
     if ((long long)nb * bs <= 600 && !first) break;
-    cur.nagg = aggregate(nb, cur.rowptr, cur.col, cur.agg);
+    cur.nagg = aggregate(nb, cur.grp, cur.gcl, cur.agg);
     if (cur.nagg >= nb || (long long)cur.nagg * 6 >= (long long)nb * bs) break;
-    cur.aptr.assign(cur.nagg + 1, 0);
-    for (int n = 0; n < nb; ++n) cur.aptr[cur.agg[n] + 1]++;
-    for (int a = 0; a < cur.nagg; ++a) cur.aptr[a + 1] += cur.aptr[a];
-    cur.amem.assign(nb, 0);
+    const int na = cur.nagg;
+    std::vector<int> aptr(na + 1, 0), amem(nb);
+    for (int n = 0; n < nb; ++n) aptr[cur.agg[n] + 1]++;
+    for (int a = 0; a < na; ++a) aptr[a + 1] += aptr[a];
     {
-      std::vector<int> f(cur.aptr.begin(), cur.aptr.end() - 1);
-      for (int n = 0; n < nb; ++n) cur.amem[f[cur.agg[n]]++] = n;
+      std::vector<int> f(aptr.begin(), aptr.end() - 1);
+      for (int n = 0; n < nb; ++n) amem[f[cur.agg[n]]++] = n;
     }
+    // tentative prolongator: per-aggregate QR of the near-null-space block
     cur.T.assign((size_t)nb * bs * 6, 0.0);
-    std::vector<double> Bc((size_t)cur.nagg * 36, 0.0);
-    for (int a = 0; a < cur.nagg; ++a) {
-      const int m = cur.aptr[a + 1] - cur.aptr[a];
+    std::vector<double> Bc((size_t)na * 36, 0.0);
+    par_for(na, [&](long long a) {
+      const int m = aptr[a + 1] - aptr[a];
       std::vector<double> M((size_t)m * bs * 6);
       if (first) {
-        double cx = 0, cy = 0, cz = 0;
-        for (int k = cur.aptr[a]; k < cur.aptr[a + 1]; ++k) {
-          const int n = cur.amem[k];
-          cx += c->X[n * 3]; cy += c->X[n * 3 + 1]; cz += c->X[n * 3 + 2];
-        }
-        cx /= m; cy /= m; cz /= m;
+        // One global centre for every aggregate: the six columns must be the
+        // same six rigid-body modes everywhere, or the coarse near-null-space
+        // (the R factors) stops describing rigid motion on the next level.
+        const double cx = ctr[0], cy = ctr[1], cz = ctr[2];
         for (int q = 0; q < m; ++q) {
-          const int n = cur.amem[cur.aptr[a] + q];
+          const int n = amem[aptr[a] + q];
           const double x = c->X[n * 3] - cx, y = c->X[n * 3 + 1] - cy, z = c->X[n * 3 + 2] - cz;
           double* r0 = &M[(q * 3 + 0) * 6];
           double* r1 = &M[(q * 3 + 1) * 6];
@@ -335,44 +353,106 @@ void build_amg_structure(pfem_ctx* c) {
         }
       } else {
         for (int q = 0; q < m; ++q) {
-          const int n = cur.amem[cur.aptr[a] + q];
+          const int n = amem[aptr[a] + q];
           for (int i = 0; i < bs * 6; ++i) M[(size_t)q * bs * 6 + i] = B[(size_t)n * bs * 6 + i];
         }
       }
       double R[36];
       mgs_qr(m * bs, M, R);
       for (int q = 0; q < m; ++q) {
-        const int n = cur.amem[cur.aptr[a] + q];
+        const int n = amem[aptr[a] + q];
         for (int i = 0; i < bs * 6; ++i) cur.T[(size_t)n * bs * 6 + i] = M[(size_t)q * bs * 6 + i];
       }
       for (int i = 0; i < 36; ++i) Bc[(size_t)a * 36 + i] = R[i];
-    }
-    // coarse pattern + fine->coarse block map
-    std::vector<std::vector<int>> cadj(cur.nagg);
+    });
+    // P pattern: row n -> aggregates of its matrix neighbours
+    std::vector<std::vector<int>> rows(nb);
+    par_for(nb, [&](long long n) {
+      auto& v = rows[n];
+      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) v.push_back(cur.agg[cur.col[k]]);
+      sorted_union(v);
+    });
+    cur.p_rp.assign(nb + 1, 0);
+    for (int n = 0; n < nb; ++n) cur.p_rp[n + 1] = cur.p_rp[n] + (int)rows[n].size();
+    cur.p_cl.resize(cur.p_rp[nb]);
+    cur.p_row.resize(cur.p_rp[nb]);
     for (int n = 0; n < nb; ++n)
-      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) cadj[cur.agg[n]].push_back(cur.agg[cur.col[k]]);
-    HostLevel nxt;
-    nxt.nbrow = cur.nagg;
-    nxt.bs = 6;
-    nxt.rowptr.assign(cur.nagg + 1, 0);
-    for (int a = 0; a < cur.nagg; ++a) {
-      auto& v = cadj[a];
-      std::sort(v.begin(), v.end());
-      v.erase(std::unique(v.begin(), v.end()), v.end());
-      nxt.rowptr[a + 1] = nxt.rowptr[a] + (int)v.size();
-    }
-    nxt.col.resize(nxt.rowptr[cur.nagg]);
-    for (int a = 0; a < cur.nagg; ++a) std::copy(cadj[a].begin(), cadj[a].end(), nxt.col.begin() + nxt.rowptr[a]);
-    cur.f2c.resize(cur.rowptr[nb]);
-    for (int n = 0; n < nb; ++n) {
-      const int I = cur.agg[n];
-      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) {
-        const int J = cur.agg[cur.col[k]];
-        const int* b0 = nxt.col.data() + nxt.rowptr[I];
-        const int* b1 = nxt.col.data() + nxt.rowptr[I + 1];
-        cur.f2c[k] = nxt.rowptr[I] + (int)(std::lower_bound(b0, b1, J) - b0);
+      for (size_t t = 0; t < rows[n].size(); ++t) {
+        cur.p_cl[cur.p_rp[n] + t] = rows[n][t];
+        cur.p_row[cur.p_rp[n] + t] = n;
       }
+    cur.pslot.resize(cur.rowptr[nb]);
+    par_for(nb, [&](long long n) {
+      const int* b0 = cur.p_cl.data() + cur.p_rp[n];
+      const int* b1 = cur.p_cl.data() + cur.p_rp[n + 1];
+      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k)
+        cur.pslot[k] = cur.p_rp[n] + (int)(std::lower_bound(b0, b1, cur.agg[cur.col[k]]) - b0);
+    });
+    // P^T
+    cur.pt_rp.assign(na + 1, 0);
+    for (int v : cur.p_cl) cur.pt_rp[v + 1]++;
+    for (int a = 0; a < na; ++a) cur.pt_rp[a + 1] += cur.pt_rp[a];
+    cur.pt_blk.resize(cur.p_cl.size());
+    {
+      std::vector<int> f(cur.pt_rp.begin(), cur.pt_rp.end() - 1);
+      for (int p = 0; p < (int)cur.p_cl.size(); ++p) cur.pt_blk[f[cur.p_cl[p]]++] = p;
     }
+    // A P pattern: row n -> union of the P rows of its neighbours
+    par_for(nb, [&](long long n) {
+      std::vector<int> v;
+      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) {
+        const int m = cur.col[k];
+        v.insert(v.end(), cur.p_cl.begin() + cur.p_rp[m], cur.p_cl.begin() + cur.p_rp[m + 1]);
+      }
+      sorted_union(v);
+      rows[n].swap(v);
+    });
+    cur.ap_rp.assign(nb + 1, 0);
+    for (int n = 0; n < nb; ++n) cur.ap_rp[n + 1] = cur.ap_rp[n] + (int)rows[n].size();
+    cur.ap_cl.resize(cur.ap_rp[nb]);
+    cur.ap_row.resize(cur.ap_rp[nb]);
+    for (int n = 0; n < nb; ++n)
+      for (size_t t = 0; t < rows[n].size(); ++t) {
+        cur.ap_cl[cur.ap_rp[n] + t] = rows[n][t];
+        cur.ap_row[cur.ap_rp[n] + t] = n;
+      }
+    rows.clear();
+    // Galerkin pattern of the next level: row I -> union of the AP rows of P^T(I)
+    std::vector<std::vector<int>> crow(na);
+    par_for(na, [&](long long I) {
+      auto& v = crow[I];
+      for (int t = cur.pt_rp[I]; t < cur.pt_rp[I + 1]; ++t) {
+        const int n = cur.p_row[cur.pt_blk[t]];
+        v.insert(v.end(), cur.ap_cl.begin() + cur.ap_rp[n], cur.ap_cl.begin() + cur.ap_rp[n + 1]);
+      }
+      sorted_union(v);
+    });
+    HostLevel nxt;
+    nxt.nbrow = na;
+    nxt.bs = 6;
+    nxt.rowptr.assign(na + 1, 0);
+    for (int a = 0; a < na; ++a) nxt.rowptr[a + 1] = nxt.rowptr[a] + (int)crow[a].size();
+    nxt.col.resize(nxt.rowptr[na]);
+    cur.c_row.resize(nxt.rowptr[na]);
+    for (int a = 0; a < na; ++a)
+      for (size_t t = 0; t < crow[a].size(); ++t) {
+        nxt.col[nxt.rowptr[a] + t] = crow[a][t];
+        cur.c_row[nxt.rowptr[a] + t] = a;
+      }
+    // aggregation graph of the next level: aggregates adjacent in this graph
+    std::vector<std::vector<int>> gadj(na);
+    par_for(na, [&](long long a) {
+      auto& v = gadj[a];
+      for (int k = aptr[a]; k < aptr[a + 1]; ++k) {
+        const int n = amem[k];
+        for (int q = cur.grp[n]; q < cur.grp[n + 1]; ++q) v.push_back(cur.agg[cur.gcl[q]]);
+      }
+      sorted_union(v);
+    });
+    nxt.grp.assign(na + 1, 0);
+    for (int a = 0; a < na; ++a) nxt.grp[a + 1] = nxt.grp[a] + (int)gadj[a].size();
+    nxt.gcl.resize(nxt.grp[na]);
+    for (int a = 0; a < na; ++a) std::copy(gadj[a].begin(), gadj[a].end(), nxt.gcl.begin() + nxt.grp[a]);
     c->hl.push_back(std::move(cur));
     cur = std::move(nxt);
     B = std::move(Bc);
@@ -432,10 +512,10 @@ template <typename T>
 int amg_alloc(pfem_ctx* ctx) {
   Amg<T>& A = amg_of<T>(ctx);
   if (!A.lv.empty()) return PFEM_OK;
-  const int L = (int)ctx->hl.size();
-  if (L < 2) return fail(ctx, PFEM_ERR_STATE, "mesh too small to build an aggregation hierarchy");
-  A.lv.resize(L - 1);
-  for (int l = 0; l < L - 1; ++l) {
+  const int L = (int)ctx->hl.size() - 1;
+  if (L < 1) return fail(ctx, PFEM_ERR_STATE, "mesh too small to build an aggregation hierarchy");
+  A.lv.resize(L);
+  for (int l = 0; l < L; ++l) {
     const HostLevel& h = ctx->hl[l];
     AmgLevel<T>& v = A.lv[l];
     v.A.nbrow = h.nbrow;
@@ -452,17 +532,25 @@ int amg_alloc(pfem_ctx* ctx) {
     CK(dalloc(ctx, &v.dinv, (size_t)h.nbrow * h.bs * h.bs));
     v.nagg = h.nagg;
     CK(upload(ctx, &v.agg, h.agg));
-    CK(upload(ctx, &v.agg_ptr, h.aptr));
-    CK(upload(ctx, &v.agg_mem, h.amem));
-    CK(upload(ctx, &v.fine2coarse, h.f2c));
     std::vector<T> Th(h.T.begin(), h.T.end());
     CK(upload(ctx, &v.T, Th));
+    v.nnzP = (int)h.p_cl.size();
+    CK(upload(ctx, &v.p_rp, h.p_rp)); CK(upload(ctx, &v.p_cl, h.p_cl)); CK(upload(ctx, &v.p_row, h.p_row));
+    CK(upload(ctx, &v.pslot, h.pslot)); CK(upload(ctx, &v.pt_rp, h.pt_rp)); CK(upload(ctx, &v.pt_blk, h.pt_blk));
+    CK(dalloc(ctx, &v.p_val, (size_t)v.nnzP * h.bs * 6));
+    v.nnzAP = (int)h.ap_cl.size();
+    CK(upload(ctx, &v.ap_rp, h.ap_rp)); CK(upload(ctx, &v.ap_cl, h.ap_cl)); CK(upload(ctx, &v.ap_row, h.ap_row));
+    CK(dalloc(ctx, &v.ap_val, (size_t)v.nnzAP * h.bs * 6));
+    CK(upload(ctx, &v.c_row, h.c_row));
+    CK(upload(ctx, &v.c_cl, ctx->hl[l + 1].col));
     const size_t n = (size_t)h.nbrow * h.bs;
     CK(dalloc(ctx, &v.x, n)); CK(dalloc(ctx, &v.b, n)); CK(dalloc(ctx, &v.r, n));
     CK(dalloc(ctx, &v.d, n)); CK(dalloc(ctx, &v.t, n));
   }
-  const HostLevel& hc = ctx->hl[L - 1];
+  const HostLevel& hc = ctx->hl[L];
   A.coarse_n = hc.nbrow * hc.bs;
+  A.coarse_nnzb = hc.rowptr[hc.nbrow];
+  CK(dalloc(ctx, &A.coarse_val, (size_t)A.coarse_nnzb * 36));
   CK(dalloc(ctx, &A.coarse_inv, (size_t)A.coarse_n * A.coarse_n));
   CK(dalloc(ctx, &A.cx, (size_t)A.coarse_n));
   CK(dalloc(ctx, &A.cb, (size_t)A.coarse_n));
@@ -538,49 +626,35 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     CKL();
     // power iteration on D^-1 A
     const long long n = (long long)v.A.nbrow * v.A.bs;
-    hash_fill_kernel<<<256, 256, 0, ctx->st>>>(n, std::is_same<T, float>::value ? (float*)v.d : nullptr,
+    pfem::count_launch(); hash_fill_kernel<<<256, 256, 0, ctx->st>>>(n, std::is_same<T, float>::value ? (float*)v.d : nullptr,
                                                std::is_same<T, double>::value ? (double*)v.d : nullptr);
     for (int it = 0; it < 12; ++it) {
       bsr_spmv<T>(v.A, v.d, v.t, ctx->st);
       blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, v.t, v.r, T(1), nullptr, ctx->st);
       dot<T>(n, v.r, v.r, w.sc + 8, w.part, ctx->st, true);
-      scale_by_inv_kernel<T><<<256, 256, 0, ctx->st>>>(n, w.sc + 8, v.r, v.d);
+      pfem::count_launch(); scale_by_inv_kernel<T><<<256, 256, 0, ctx->st>>>(n, w.sc + 8, v.r, v.d);
     }
     CKL();
     T lm = 0;
     CK(cudaMemcpyAsync(&lm, w.sc + 8, sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     v.lmax = (T)(1.1 * (double)lm);
-    // Galerkin coarse operator
-    T* cval;
-    long long cnnzb;
-    if (l + 1 < L) {
-      cval = A.lv[l + 1].A.val;
-      cnnzb = A.lv[l + 1].A.nnzb;
-    } else {
-      cval = A.lv[l].t;  // placeholder; coarsest handled below
-      cnnzb = 0;
-    }
-    if (l + 1 < L) {
-      CK(cudaMemsetAsync(cval, 0, (size_t)cnnzb * 36 * sizeof(T), ctx->st));
-      galerkin<T>(v.A, v.T, v.fine2coarse, cval, ctx->st);
-      CKL();
-    }
+    if (getenv("PFEM_DEBUG_AMG"))
+      fprintf(stderr, "amg level %d: block rows %d bs %d nnzb %lld aggregates %d P blocks %d lmax %.4g\n", l,
+              v.A.nbrow, v.A.bs, v.A.nnzb, v.nagg, v.nnzP, (double)v.lmax);
+    // smoothed prolongator and Galerkin operator of the next level
+    const T omega = (T)(4.0 / (3.0 * (double)lm));
+    T* cval = (l + 1 < L) ? A.lv[l + 1].A.val : A.coarse_val;
+    const int nnzC = (int)ctx->hl[l + 1].rowptr[ctx->hl[l + 1].nbrow];
+    sa_setup_level<T>(v, omega, cval, nnzC, ctx->st);
+    CKL();
   }
-  // coarsest operator: Galerkin product into a host-side dense matrix
+  // coarsest operator: dense inverse on the host (a few hundred dofs)
   {
     const HostLevel& hc = ctx->hl[L];
-    const AmgLevel<T>& v = A.lv[L - 1];
-    const long long cnnzb = hc.rowptr[hc.nbrow];
-    T* cval = nullptr;
-    CK(cudaMalloc((void**)&cval, (size_t)std::max<long long>(cnnzb, 1) * 36 * sizeof(T)));
-    CK(cudaMemsetAsync(cval, 0, (size_t)cnnzb * 36 * sizeof(T), ctx->st));
-    galerkin<T>(v.A, v.T, v.fine2coarse, cval, ctx->st);
-    CKL();
-    std::vector<T> hv((size_t)cnnzb * 36);
-    CK(cudaMemcpyAsync(hv.data(), cval, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
+    std::vector<T> hv((size_t)A.coarse_nnzb * 36);
+    CK(cudaMemcpyAsync(hv.data(), A.coarse_val, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    cudaFree(cval);
     const int n = A.coarse_n;
     std::vector<double> dense((size_t)n * n, 0.0), inv;
     for (int I = 0; I < hc.nbrow; ++I)
@@ -642,10 +716,10 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
   bsr_residual<T>(v.A, x, b, v.t, ctx->st);
   T* bn = (l + 1 < L) ? A.lv[l + 1].b : A.cb;
   T* xn = (l + 1 < L) ? A.lv[l + 1].x : A.cx;
-  amg_restrict<T>(v.nagg, v.A.bs, v.agg_ptr, v.agg_mem, v.T, v.t, bn, ctx->st);
+  sa_restrict<T>(v, v.t, bn, ctx->st);
   if (l + 1 < L) vcycle<T>(ctx, l + 1, bn, xn);
   else dense_mv<T>(A.coarse_n, A.coarse_inv, bn, xn, ctx->st);
-  amg_prolong<T>(v.A.nbrow, v.A.bs, v.agg, v.T, xn, x, ctx->st);
+  sa_prolong<T>(v, xn, x, ctx->st);
   cheb<T>(ctx, v, A.cheb_degree, b, x, false);
 }
 
@@ -692,7 +766,7 @@ int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* 
     CK(cudaMemcpyAsync(w.rh, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
     fill<T>(n, w.v, T(0), st);
     fill<T>(n, w.p, T(0), st);
-    bicg_init_kernel<T><<<1, 1, 0, st>>>(w.sc);
+    pfem::count_launch(); bicg_init_kernel<T><<<1, 1, 0, st>>>(w.sc);
     for (int it = 1; it <= itmax; ++it) {
       dot<T>(n, w.rh, w.r, w.sc + 0, w.part, st, false);
       bicg_p<T>(n, w.sc, w.r, w.v, w.p, st);
@@ -705,7 +779,7 @@ int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* 
       dot<T>(n, w.t, w.s, w.sc + 5, w.part, st, false);
       dot<T>(n, w.t, w.t, w.sc + 6, w.part, st, false);
       bicg_xr<T>(n, w.sc, w.ph, w.sh, w.s, w.t, w.x, w.r, st);
-      bicg_finish_kernel<T><<<1, 1, 0, st>>>(w.sc);
+      pfem::count_launch(); bicg_finish_kernel<T><<<1, 1, 0, st>>>(w.sc);
       dot<T>(n, w.r, w.r, w.sc + 3, w.part, st, true);
       T rn = 0;
       CK(cudaMemcpyAsync(&rn, w.sc + 3, sizeof(T), cudaMemcpyDeviceToHost, st));
@@ -905,6 +979,7 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     CK(cudaMemcpyAsync(ctx->dUtmp, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
     double a = 1.0, rt = 0.0;
     for (int bt = 0;; ++bt) {
+      pfem::count_launch();
       if (o->precision == PFEM_FP64)
         step_kernel<double><<<1024, 256, 0, ctx->st>>>(ctx->ndof, a, ctx->kw64.x, ctx->dUtmp, ctx->dU);
       else
@@ -951,6 +1026,43 @@ __global__ void init_state_kernel(long long ngp, double* cpi, double* alpha, dou
 }
 
 }  // namespace
+
+template <typename T>
+static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t* dims) {
+  Amg<T>& A = amg_of<T>(ctx);
+  const int L = (int)A.lv.size();
+  if (!A.built || level < 0 || level > L || (what == 1 && level >= L))
+    return fail(ctx, PFEM_ERR_BAD_ARG, "no such AMG level");
+  const HostLevel& h = ctx->hl[level];
+  const int bs = h.bs, nr = h.nbrow * bs;
+  if (what == 0) {
+    if (dims) { dims[0] = nr; dims[1] = nr; }
+    if (!out) return PFEM_OK;
+    const long long nb = h.rowptr[h.nbrow];
+    std::vector<T> v((size_t)nb * bs * bs);
+    const T* src = level < L ? A.lv[level].A.val : A.coarse_val;
+    CK(cudaMemcpy(v.data(), src, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    std::fill(out, out + (size_t)nr * nr, 0.0);
+    for (int I = 0; I < h.nbrow; ++I)
+      for (int k = h.rowptr[I]; k < h.rowptr[I + 1]; ++k)
+        for (int r = 0; r < bs; ++r)
+          for (int c = 0; c < bs; ++c)
+            out[(size_t)(I * bs + r) * nr + h.col[k] * bs + c] = (double)v[(size_t)k * bs * bs + r * bs + c];
+  } else {
+    const int nc = h.nagg * 6;
+    if (dims) { dims[0] = nr; dims[1] = nc; }
+    if (!out) return PFEM_OK;
+    std::vector<T> v((size_t)h.p_cl.size() * bs * 6);
+    CK(cudaMemcpy(v.data(), A.lv[level].p_val, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    std::fill(out, out + (size_t)nr * nc, 0.0);
+    for (int n = 0; n < h.nbrow; ++n)
+      for (int p = h.p_rp[n]; p < h.p_rp[n + 1]; ++p)
+        for (int i = 0; i < bs; ++i)
+          for (int c = 0; c < 6; ++c)
+            out[(size_t)(n * bs + i) * nc + h.p_cl[p] * 6 + c] = (double)v[(size_t)p * bs * 6 + i * 6 + c];
+  }
+  return PFEM_OK;
+}
 
 // =====================================================================  C ABI
 extern "C" {
@@ -1028,6 +1140,8 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     if (e != cudaSuccess) { pfem_set_cuda_error(e, "cudaStreamCreate", __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
     cudaEventCreate(&ctx->e0);
     cudaEventCreate(&ctx->e1);
+    cudaEventCreate(&ctx->t0);
+    cudaEventCreate(&ctx->t1);
   }
   if ((long long)ctx->ndof >= (1ll << 31)) return bail(fail(ctx, PFEM_ERR_BAD_ARG, "mesh too large for 32-bit dof indices"));
   // ---- host topology ----
@@ -1146,6 +1260,8 @@ void pfem_destroy(pfem_ctx* ctx) {
   pfem::mlp_free(ctx->mlp);
   if (ctx->e0) cudaEventDestroy(ctx->e0);
   if (ctx->e1) cudaEventDestroy(ctx->e1);
+  if (ctx->t0) cudaEventDestroy(ctx->t0);
+  if (ctx->t1) cudaEventDestroy(ctx->t1);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
 }
@@ -1292,7 +1408,7 @@ int pfem_reset(pfem_ctx* ctx) {
   if (!ctx) return PFEM_ERR_BAD_ARG;
   if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
   cudaSetDevice(ctx->device);
-  init_state_kernel<<<1024, 256, 0, ctx->st>>>(ctx->ngp, ctx->dCpi, ctx->dAlpha, ctx->dEpsp, ctx->dTau);
+  pfem::count_launch(); init_state_kernel<<<1024, 256, 0, ctx->st>>>(ctx->ngp, ctx->dCpi, ctx->dAlpha, ctx->dEpsp, ctx->dTau);
   CKL();
   CK(cudaMemsetAsync(ctx->dFlags, 0, ctx->ngp, ctx->st));
   CK(cudaMemsetAsync(ctx->dU, 0, ctx->ndof * sizeof(double), ctx->st));
@@ -1380,7 +1496,7 @@ static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepT
   if (o->predictor != PFEM_PRED_PREVIOUS && ctx->steps_taken >= 1) {
     const double dl = ctx->lam_prev - ctx->lam_prev2;
     const double f = dl > 0 ? (lam - ctx->lam_prev) / dl : 0.0;
-    extrap_kernel<<<1024, 256, 0, ctx->st>>>(n, f, ctx->dUprev, ctx->dUprev2, ctx->dU);
+    pfem::count_launch(); extrap_kernel<<<1024, 256, 0, ctx->st>>>(n, f, ctx->dUprev, ctx->dUprev2, ctx->dU);
     bc_apply(ctx->bc, lam, ctx->dU, ctx->st);
     CKL();
   }
@@ -1467,6 +1583,19 @@ int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res, 
   return r.converged ? PFEM_OK : fail(ctx, PFEM_ERR_NOT_CONVERGED, "a load step did not converge");
 }
 
+int pfem_residual(pfem_ctx* ctx, double lambda, int32_t precision, double* rnorm, double* R) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  if (!ctx->bcs_set) return fail(ctx, PFEM_ERR_STATE, "pfem_set_bcs must be called first");
+  cudaSetDevice(ctx->device);
+  double rn = 0, t = 0;
+  int rc = residual_system(ctx, precision == PFEM_MIXED ? PFEM_MIXED : PFEM_FP64, lambda, &rn, &t);
+  if (rc) return rc;
+  if (rnorm) *rnorm = rn;
+  if (R) CK(cudaMemcpy(R, ctx->dR, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  return PFEM_OK;
+}
+
 int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, int32_t rebuild_pc,
                       const pfem_solve_opts* o, int32_t* niter) {
   if (!ctx || !b || !x || !o) return PFEM_ERR_BAD_ARG;
@@ -1498,6 +1627,37 @@ int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, in
   }
   if (niter) *niter = it;
   return conv ? PFEM_OK : fail(ctx, PFEM_ERR_LINSOLVE, "Krylov solve did not reach its tolerance");
+}
+
+int pfem_amg_apply(pfem_ctx* ctx, const double* r, double* z) {
+  if (!ctx || !r || !z) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  const long long n = ctx->ndof;
+  if (ctx->tangent_prec == PFEM_FP64 && ctx->amg64.built) {
+    CK(cudaMemcpy(ctx->kw64.r, r, n * sizeof(double), cudaMemcpyHostToDevice));
+    vcycle<double>(ctx, 0, ctx->kw64.r, ctx->kw64.z);
+    CKL();
+    CK(cudaMemcpy(z, ctx->kw64.z, n * sizeof(double), cudaMemcpyDeviceToHost));
+  } else if (ctx->tangent_prec == PFEM_MIXED && ctx->amg32.built) {
+    std::vector<float> f(r, r + n);
+    CK(cudaMemcpy(ctx->kw32.r, f.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    vcycle<float>(ctx, 0, ctx->kw32.r, ctx->kw32.z);
+    CKL();
+    CK(cudaMemcpy(f.data(), ctx->kw32.z, n * sizeof(float), cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < n; ++i) z[i] = f[i];
+  } else {
+    return fail(ctx, PFEM_ERR_STATE, "no AMG hierarchy built for the resident tangent");
+  }
+  return PFEM_OK;
+}
+
+int pfem_amg_dense(pfem_ctx* ctx, int32_t level, int32_t what, double* out, int64_t* dims) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  if (ctx->tangent_prec == PFEM_MIXED) return amg_dense_t<float>(ctx, level, what, out, dims);
+  return amg_dense_t<double>(ctx, level, what, out, dims);
 }
 
 int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, double* cpi, double* epsp,
@@ -1615,6 +1775,24 @@ int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms) {
   float t = 0;
   CK(cudaEventElapsedTime(&t, ctx->e0, ctx->e1));
   *ms = t / reps;
+  return PFEM_OK;
+}
+
+int64_t pfem_kernel_launches(void) { return (int64_t)g_launches; }
+
+int pfem_timer(pfem_ctx* ctx, int32_t op, double* ms) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  if (op == 0) {
+    CK(cudaEventRecord(ctx->t0, ctx->st));
+    return PFEM_OK;
+  }
+  CK(cudaEventRecord(ctx->t1, ctx->st));
+  CK(cudaEventSynchronize(ctx->t1));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, ctx->t0, ctx->t1));
+  if (ms) *ms = t;
   return PFEM_OK;
 }
 

@@ -17,6 +17,11 @@ void pfem_set_cuda_error(cudaError_t e, const char* what, const char* file, int 
 
 namespace pfem {
 
+// Process-wide count of kernel launches made by this library (every launch
+// site calls count_launch() once), read through pfem_kernel_launches().
+long long& launch_counter();
+inline void count_launch() { ++launch_counter(); }
+
 // Material constants with the derived moduli of J2Material
 // (lagrangian/src/Materials.jl:104-107).
 struct MatParams {

@@ -471,7 +471,7 @@ static void launch_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     attr = true;
   }
-  element_color_kernel<KT, COMMIT, FBAR><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
+  pfem::count_launch(); element_color_kernel<KT, COMMIT, FBAR><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
 }
 
 template <typename KT>

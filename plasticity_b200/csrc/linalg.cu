@@ -71,6 +71,7 @@ template <typename T>
 void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st) {
   const long long threads = (long long)A.nbrow * 32;
   const int blocks = (int)((threads + 255) / 256);
+  pfem::count_launch();
   if (A.bs == 3)
     bsr_spmv_kernel<T, 3, 0><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, nullptr, nullptr, nullptr);
   else
@@ -80,6 +81,7 @@ template <typename T>
 void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t st) {
   const long long threads = (long long)A.nbrow * 32;
   const int blocks = (int)((threads + 255) / 256);
+  pfem::count_launch();
   if (A.bs == 3)
     bsr_spmv_kernel<T, 3, 1><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, r, b, nullptr, nullptr);
   else
@@ -89,6 +91,7 @@ template <typename T>
 void bsr_cheb_step(const BsrMat<T>& A, const T* dinv, const T* d, T* r, T* x, cudaStream_t st) {
   const long long threads = (long long)A.nbrow * 32;
   const int blocks = (int)((threads + 255) / 256);
+  pfem::count_launch();
   if (A.bs == 3)
     bsr_spmv_kernel<T, 3, 2><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, d, r, nullptr, dinv, x);
   else
@@ -116,8 +119,8 @@ template <typename T>
 void blockdiag_apply(int nbrow, int bs, const T* dinv, const T* v, T* r, T scale, T* d, cudaStream_t st) {
   const long long n = (long long)nbrow * bs;
   const int blocks = (int)((n + 255) / 256);
-  if (bs == 3) blockdiag_apply_kernel<T, 3><<<blocks, 256, 0, st>>>(nbrow, dinv, v, r, scale, d);
-  else blockdiag_apply_kernel<T, 6><<<blocks, 256, 0, st>>>(nbrow, dinv, v, r, scale, d);
+  if (bs == 3) { pfem::count_launch(); blockdiag_apply_kernel<T, 3><<<blocks, 256, 0, st>>>(nbrow, dinv, v, r, scale, d); }
+  else { pfem::count_launch(); blockdiag_apply_kernel<T, 6><<<blocks, 256, 0, st>>>(nbrow, dinv, v, r, scale, d); }
 }
 
 // Invert the diagonal blocks (Gauss-Jordan with partial pivoting in double).
@@ -172,8 +175,8 @@ __global__ void blockdiag_invert_kernel(int nbrow, const int* __restrict__ rowpt
 template <typename T>
 void blockdiag_invert(const BsrMat<T>& A, T* dinv, cudaStream_t st) {
   const int blocks = (A.nbrow + 127) / 128;
-  if (A.bs == 3) blockdiag_invert_kernel<T, 3><<<blocks, 128, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, dinv);
-  else blockdiag_invert_kernel<T, 6><<<blocks, 128, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, dinv);
+  if (A.bs == 3) { pfem::count_launch(); blockdiag_invert_kernel<T, 3><<<blocks, 128, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, dinv); }
+  else { pfem::count_launch(); blockdiag_invert_kernel<T, 6><<<blocks, 128, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, dinv); }
 }
 
 // ------------------------------------------------------------------ reductions
@@ -219,8 +222,8 @@ template <typename T>
 void dot(long long n, const T* a, const T* b, T* out, T* part, cudaStream_t st, bool take_sqrt) {
   long long nb = (n + RED_THREADS - 1) / RED_THREADS;
   const int blocks = (int)(nb < RED_BLOCKS ? (nb > 0 ? nb : 1) : RED_BLOCKS);
-  dot_partial_kernel<T><<<blocks, RED_THREADS, 0, st>>>(n, a, b, part);
-  sum_final_kernel<T><<<1, 1024, 0, st>>>(blocks, part, out, take_sqrt ? 1 : 0);
+  pfem::count_launch(); dot_partial_kernel<T><<<blocks, RED_THREADS, 0, st>>>(n, a, b, part);
+  pfem::count_launch(); sum_final_kernel<T><<<1, 1024, 0, st>>>(blocks, part, out, take_sqrt ? 1 : 0);
 }
 
 // ------------------------------------------------------------------ vector ops
@@ -232,7 +235,7 @@ __global__ void fill_kernel(long long n, T* x, T v) {
 template <typename T>
 void fill(long long n, T* x, T v, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  if (n > 0) fill_kernel<T><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(n, x, v);
+  if (n > 0) { pfem::count_launch(); fill_kernel<T><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(n, x, v); }
 }
 // y = a*x + b*y with host scalars
 template <typename T>
@@ -243,7 +246,7 @@ __global__ void axpby_kernel(long long n, T a, const T* __restrict__ x, T b, T* 
 template <typename T>
 void axpby(long long n, T a, const T* x, T b, T* y, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  if (n > 0) axpby_kernel<T><<<blocks, 256, 0, st>>>(n, a, x, b, y);
+  if (n > 0) { pfem::count_launch(); axpby_kernel<T><<<blocks, 256, 0, st>>>(n, a, x, b, y); }
 }
 // CG update with device scalars: alpha = num/den;  x += alpha p;  r -= alpha q
 template <typename T>
@@ -259,7 +262,7 @@ __global__ void cg_xr_kernel(long long n, const T* __restrict__ num, const T* __
 template <typename T>
 void cg_xr(long long n, const T* num, const T* den, const T* p, const T* q, T* x, T* r, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  cg_xr_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, p, q, x, r);
+  pfem::count_launch(); cg_xr_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, p, q, x, r);
 }
 // p = z + (num/den) p
 template <typename T>
@@ -272,7 +275,7 @@ __global__ void cg_p_kernel(long long n, const T* __restrict__ num, const T* __r
 template <typename T>
 void cg_p(long long n, const T* num, const T* den, const T* z, T* p, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  cg_p_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, z, p);
+  pfem::count_launch(); cg_p_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, z, p);
 }
 // BiCGStab helpers with device scalars s[0..]: see krylov code for layout.
 template <typename T>
@@ -287,7 +290,7 @@ __global__ void bicg_p_kernel(long long n, const T* __restrict__ sc, const T* __
 template <typename T>
 void bicg_p(long long n, const T* sc, const T* r, const T* v, T* p, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  bicg_p_kernel<T><<<blocks, 256, 0, st>>>(n, sc, r, v, p);
+  pfem::count_launch(); bicg_p_kernel<T><<<blocks, 256, 0, st>>>(n, sc, r, v, p);
 }
 // s = r - alpha v  (alpha = sc[0]/sc[4])
 template <typename T>
@@ -300,7 +303,7 @@ __global__ void bicg_s_kernel(long long n, const T* __restrict__ sc, const T* __
 template <typename T>
 void bicg_s(long long n, const T* sc, const T* r, const T* v, T* s, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  bicg_s_kernel<T><<<blocks, 256, 0, st>>>(n, sc, r, v, s);
+  pfem::count_launch(); bicg_s_kernel<T><<<blocks, 256, 0, st>>>(n, sc, r, v, s);
 }
 // x += alpha ph + omega sh;  r = s - omega t  (alpha = sc[0]/sc[4], omega = sc[5]/sc[6])
 template <typename T>
@@ -318,13 +321,16 @@ template <typename T>
 void bicg_xr(long long n, const T* sc, const T* ph, const T* sh, const T* s, const T* t, T* x, T* r,
              cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  bicg_xr_kernel<T><<<blocks, 256, 0, st>>>(n, sc, ph, sh, s, t, x, r);
+  pfem::count_launch(); bicg_xr_kernel<T><<<blocks, 256, 0, st>>>(n, sc, ph, sh, s, t, x, r);
 }
 // scalar bookkeeping: dst[i] = src[j]
 template <typename T>
 __global__ void scalar_copy_kernel(T* dst, const T* src) { *dst = *src; }
 template <typename T>
-void scalar_copy(T* dst, const T* src, cudaStream_t st) { scalar_copy_kernel<T><<<1, 1, 0, st>>>(dst, src); }
+void scalar_copy(T* dst, const T* src, cudaStream_t st) {
+  pfem::count_launch();
+  scalar_copy_kernel<T><<<1, 1, 0, st>>>(dst, src);
+}
 
 // precision conversion
 template <typename A, typename B>
@@ -335,7 +341,7 @@ __global__ void convert_kernel(long long n, const A* __restrict__ a, B* __restri
 template <typename A, typename B>
 void convert(long long n, const A* a, B* b, double s, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  convert_kernel<A, B><<<blocks, 256, 0, st>>>(n, a, b, s);
+  pfem::count_launch(); convert_kernel<A, B><<<blocks, 256, 0, st>>>(n, a, b, s);
 }
 // U += (double) x
 template <typename T>
@@ -346,7 +352,7 @@ __global__ void add_to_double_kernel(long long n, const T* __restrict__ x, doubl
 template <typename T>
 void add_to_double(long long n, const T* x, double* U, cudaStream_t st) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
-  add_to_double_kernel<T><<<blocks, 256, 0, st>>>(n, x, U);
+  pfem::count_launch(); add_to_double_kernel<T><<<blocks, 256, 0, st>>>(n, x, U);
 }
 
 // ------------------------------------------------------------------ Dirichlet (K3)
@@ -396,16 +402,16 @@ template <typename KT>
 void impose_dirichlet(const BcDev& bc, long long ndof, double lam, const double* U, KT* K, double* R,
                       double* dg, cudaStream_t st) {
   const int b1 = (int)std::min<long long>((ndof + 255) / 256, 4096);
-  residual_fext_kernel<<<b1, 256, 0, st>>>(ndof, lam, bc.fn, R);
+  pfem::count_launch(); residual_fext_kernel<<<b1, 256, 0, st>>>(ndof, lam, bc.fn, R);
   if (bc.nbc == 0) return;
-  bc_dg_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U, dg);
+  pfem::count_launch(); bc_dg_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U, dg);
   if (bc.nrows > 0)
-    bc_rhs_kernel<KT><<<(bc.nrows + 127) / 128, 128, 0, st>>>(bc.nrows, bc.rows, bc.rptr, bc.rpos, bc.rcol, K, dg, R);
+    pfem::count_launch(); bc_rhs_kernel<KT><<<(bc.nrows + 127) / 128, 128, 0, st>>>(bc.nrows, bc.rows, bc.rptr, bc.rpos, bc.rcol, K, dg, R);
   if (bc.nzero > 0) {
     const int b2 = (int)std::min<long long>((bc.nzero + 255) / 256, 4096);
-    bc_zero_kernel<KT><<<b2, 256, 0, st>>>(bc.nzero, bc.zpos, bc.zone, K);
+    pfem::count_launch(); bc_zero_kernel<KT><<<b2, 256, 0, st>>>(bc.nzero, bc.zpos, bc.zone, K);
   }
-  bc_set_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, dg, R);
+  pfem::count_launch(); bc_set_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, dg, R);
 }
 // Set U[d] = g(lambda) on constrained dofs (predictors honour the BCs).
 __global__ void bc_apply_kernel(int nbc, const int* __restrict__ dofs, const double* __restrict__ vals,
@@ -415,98 +421,10 @@ __global__ void bc_apply_kernel(int nbc, const int* __restrict__ dofs, const dou
   U[dofs[i]] = ramp[i] ? lam * vals[i] : vals[i];
 }
 void bc_apply(const BcDev& bc, double lam, double* U, cudaStream_t st) {
-  if (bc.nbc > 0) bc_apply_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U);
+  if (bc.nbc > 0) { pfem::count_launch(); bc_apply_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U); }
 }
 
-// ------------------------------------------------------------------ AMG transfer
-// Galerkin product with the tentative prolongator: for every fine block
-// (n, m):  C += T_n^T A_nm T_m  into coarse block f2c[k] (6 x 6).
-template <typename T, int BS>
-__global__ void galerkin_kernel(int nbrow, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                const T* __restrict__ val, const T* __restrict__ Tb,
-                                const int* __restrict__ f2c, T* __restrict__ cval) {
-  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= nbrow) return;
-  const T* Tn = Tb + (long long)row * BS * 6;
-  for (int k = rowptr[row] + lane; k < rowptr[row + 1]; k += 32) {
-    const int m = col[k];
-    const T* A = val + (long long)k * BS * BS;
-    const T* Tm = Tb + (long long)m * BS * 6;
-    T W[BS][6];
-#pragma unroll
-    for (int i = 0; i < BS; ++i)
-#pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        T s = T(0);
-#pragma unroll
-        for (int j = 0; j < BS; ++j) s += A[i * BS + j] * Tm[j * 6 + c];
-        W[i][c] = s;
-      }
-    T* C = cval + (long long)f2c[k] * 36;
-#pragma unroll
-    for (int r = 0; r < 6; ++r)
-#pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        T s = T(0);
-#pragma unroll
-        for (int i = 0; i < BS; ++i) s += Tn[i * 6 + r] * W[i][c];
-        atomicAdd(C + r * 6 + c, s);
-      }
-  }
-}
-template <typename T>
-void galerkin(const BsrMat<T>& A, const T* Tb, const int* f2c, T* cval, cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 32;
-  const int blocks = (int)((threads + 255) / 256);
-  if (A.bs == 3) galerkin_kernel<T, 3><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, Tb, f2c, cval);
-  else galerkin_kernel<T, 6><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, Tb, f2c, cval);
-}
-// Restriction: bc[I*6 + c] = sum_{n in I} (T_n^T r_n)_c
-template <typename T, int BS>
-__global__ void restrict_kernel(int nagg, const int* __restrict__ aptr, const int* __restrict__ amem,
-                                const T* __restrict__ Tb, const T* __restrict__ r, T* __restrict__ bc) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nagg * 6) return;
-  const int I = (int)(i / 6), c = (int)(i % 6);
-  T s = T(0);
-  for (int k = aptr[I]; k < aptr[I + 1]; ++k) {
-    const int n = amem[k];
-    const T* Tn = Tb + (long long)n * BS * 6;
-#pragma unroll
-    for (int j = 0; j < BS; ++j) s += Tn[j * 6 + c] * r[(long long)n * BS + j];
-  }
-  bc[i] = s;
-}
-template <typename T>
-void amg_restrict(int nagg, int bs, const int* aptr, const int* amem, const T* Tb, const T* r, T* bc, cudaStream_t st) {
-  const long long n = (long long)nagg * 6;
-  const int blocks = (int)((n + 255) / 256);
-  if (bs == 3) restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(nagg, aptr, amem, Tb, r, bc);
-  else restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(nagg, aptr, amem, Tb, r, bc);
-}
-// Prolongation: x_n += T_n xc[agg(n)]
-template <typename T, int BS>
-__global__ void prolong_kernel(int nbrow, const int* __restrict__ agg, const T* __restrict__ Tb,
-                               const T* __restrict__ xc, T* __restrict__ x) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nbrow * BS) return;
-  const long long n = i / BS;
-  const int j = (int)(i - n * BS);
-  const T* Tn = Tb + n * BS * 6 + j * 6;
-  const T* xa = xc + (long long)agg[n] * 6;
-  T s = T(0);
-#pragma unroll
-  for (int c = 0; c < 6; ++c) s += Tn[c] * xa[c];
-  x[i] += s;
-}
-template <typename T>
-void amg_prolong(int nbrow, int bs, const int* agg, const T* Tb, const T* xc, T* x, cudaStream_t st) {
-  const long long n = (long long)nbrow * bs;
-  const int blocks = (int)((n + 255) / 256);
-  if (bs == 3) prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(nbrow, agg, Tb, xc, x);
-  else prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(nbrow, agg, Tb, xc, x);
-}
+// ------------------------------------------------------------------ coarse solve
 // Dense coarse solve y = Ainv b (one warp per row).
 template <typename T>
 __global__ void dense_mv_kernel(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ y) {
@@ -522,7 +440,215 @@ __global__ void dense_mv_kernel(int n, const T* __restrict__ M, const T* __restr
 template <typename T>
 void dense_mv(int n, const T* M, const T* b, T* y, cudaStream_t st) {
   const int blocks = (int)(((long long)n * 32 + 255) / 256);
-  dense_mv_kernel<T><<<blocks, 256, 0, st>>>(n, M, b, y);
+  pfem::count_launch(); dense_mv_kernel<T><<<blocks, 256, 0, st>>>(n, M, b, y);
+}
+
+// ------------------------------------------------------------------ smoothed aggregation
+// P = (I - w D^-1 A) T with the tentative T (one bs x 6 block per fine row).
+// One thread per P block p (row n, aggregate J):
+//   P_p = [J == agg(n)] T_n - w Dinv_n sum_{k in row n, agg(col k) == J} A_k T_col(k)
+// pslot[k] names the P block that A block k feeds.
+template <typename T, int BS>
+__global__ void sa_prolongator_kernel(int nnzP, const int* __restrict__ p_row, const int* __restrict__ p_cl,
+                                      const int* __restrict__ rowptr, const int* __restrict__ col,
+                                      const T* __restrict__ val, const int* __restrict__ pslot,
+                                      const int* __restrict__ agg, const T* __restrict__ Tb,
+                                      const T* __restrict__ dinv, T w, T* __restrict__ pval) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nnzP) return;
+  const int n = p_row[p];
+  T acc[BS][6];
+#pragma unroll
+  for (int i = 0; i < BS; ++i)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[i][c] = T(0);
+  for (int k = rowptr[n]; k < rowptr[n + 1]; ++k) {
+    if (pslot[k] != p) continue;
+    const T* A = val + (long long)k * BS * BS;
+    const T* Tm = Tb + (long long)col[k] * BS * 6;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int j = 0; j < BS; ++j) {
+        const T a = A[i * BS + j];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[i][c] += a * Tm[j * 6 + c];
+      }
+  }
+  const T* D = dinv + (long long)n * BS * BS;
+  const bool own = p_cl[p] == agg[n];
+  const T* Tn = Tb + (long long)n * BS * 6;
+  T* P = pval + (long long)p * BS * 6;
+#pragma unroll
+  for (int i = 0; i < BS; ++i)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      T s = T(0);
+#pragma unroll
+      for (int j = 0; j < BS; ++j) s += D[i * BS + j] * acc[j][c];
+      P[i * 6 + c] = (own ? Tn[i * 6 + c] : T(0)) - w * s;
+    }
+}
+
+__device__ __forceinline__ int find_sorted(const int* __restrict__ a, int lo, int hi, int key) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = a[mid];
+    if (v == key) return mid;
+    if (v < key) lo = mid + 1; else hi = mid;
+  }
+  return -1;
+}
+
+// AP block q (row n, coarse column J) = sum_{k in row n} A_k P[col k, J].
+template <typename T, int BS>
+__global__ void sa_ap_kernel(int nnzAP, const int* __restrict__ ap_row, const int* __restrict__ ap_cl,
+                             const int* __restrict__ rowptr, const int* __restrict__ col,
+                             const T* __restrict__ val, const int* __restrict__ p_rp,
+                             const int* __restrict__ p_cl, const T* __restrict__ pval, T* __restrict__ apval) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nnzAP) return;
+  const int n = ap_row[q], J = ap_cl[q];
+  T acc[BS][6];
+#pragma unroll
+  for (int i = 0; i < BS; ++i)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[i][c] = T(0);
+  for (int k = rowptr[n]; k < rowptr[n + 1]; ++k) {
+    const int m = col[k];
+    const int p = find_sorted(p_cl, p_rp[m], p_rp[m + 1], J);
+    if (p < 0) continue;
+    const T* A = val + (long long)k * BS * BS;
+    const T* P = pval + (long long)p * BS * 6;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int j = 0; j < BS; ++j) {
+        const T a = A[i * BS + j];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[i][c] += a * P[j * 6 + c];
+      }
+  }
+  T* O = apval + (long long)q * BS * 6;
+#pragma unroll
+  for (int i = 0; i < BS; ++i)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) O[i * 6 + c] = acc[i][c];
+}
+
+// Coarse block c (I, J) = sum_{p in P^T row I} P_p^T AP[row(p), J]   (6 x 6)
+template <typename T, int BS>
+__global__ void sa_rap_kernel(int nnzC, const int* __restrict__ c_row, const int* __restrict__ c_cl,
+                              const int* __restrict__ pt_rp, const int* __restrict__ pt_blk,
+                              const int* __restrict__ p_row, const T* __restrict__ pval,
+                              const int* __restrict__ ap_rp, const int* __restrict__ ap_cl,
+                              const T* __restrict__ apval, T* __restrict__ cval) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nnzC) return;
+  const int I = c_row[c], J = c_cl[c];
+  T acc[6][6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[r][q] = T(0);
+  for (int t = pt_rp[I]; t < pt_rp[I + 1]; ++t) {
+    const int p = pt_blk[t];
+    const int n = p_row[p];
+    const int q = find_sorted(ap_cl, ap_rp[n], ap_rp[n + 1], J);
+    if (q < 0) continue;
+    const T* P = pval + (long long)p * BS * 6;
+    const T* AP = apval + (long long)q * BS * 6;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        const T pr = P[i * 6 + r];
+#pragma unroll
+        for (int q2 = 0; q2 < 6; ++q2) acc[r][q2] += pr * AP[i * 6 + q2];
+      }
+  }
+  T* O = cval + (long long)c * 36;
+#pragma unroll
+  for (int r = 0; r < 6; ++r)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) O[r * 6 + q] = acc[r][q];
+}
+
+// Restriction bc[I*6+c] = sum_{p in P^T row I} (P_p^T r_row(p))_c
+template <typename T, int BS>
+__global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, const int* __restrict__ pt_blk,
+                                   const int* __restrict__ p_row, const T* __restrict__ pval,
+                                   const T* __restrict__ r, T* __restrict__ bc) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nagg * 6) return;
+  const int I = (int)(i / 6), c = (int)(i % 6);
+  T s = T(0);
+  for (int t = pt_rp[I]; t < pt_rp[I + 1]; ++t) {
+    const int p = pt_blk[t];
+    const T* P = pval + (long long)p * BS * 6;
+    const T* rv = r + (long long)p_row[p] * BS;
+#pragma unroll
+    for (int j = 0; j < BS; ++j) s += P[j * 6 + c] * rv[j];
+  }
+  bc[i] = s;
+}
+// Prolongation x[n*BS+j] += sum_{p in P row n} (P_p xc[col(p)])_j
+template <typename T, int BS>
+__global__ void sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp, const int* __restrict__ p_cl,
+                                  const T* __restrict__ pval, const T* __restrict__ xc, T* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nbrow * BS) return;
+  const int n = (int)(i / BS), j = (int)(i % BS);
+  T s = T(0);
+  for (int p = p_rp[n]; p < p_rp[n + 1]; ++p) {
+    const T* P = pval + (long long)p * BS * 6 + j * 6;
+    const T* xa = xc + (long long)p_cl[p] * 6;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) s += P[c] * xa[c];
+  }
+  x[i] += s;
+}
+
+template <typename T>
+void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t st) {
+  const int BSs = v.A.bs;
+  if (BSs == 3) {
+    pfem::count_launch();
+    sa_prolongator_kernel<T, 3><<<(v.nnzP + 127) / 128, 128, 0, st>>>(v.nnzP, v.p_row, v.p_cl, v.A.rowptr, v.A.col,
+                                                                     v.A.val, v.pslot, v.agg, v.T, v.dinv, w, v.p_val);
+    pfem::count_launch();
+    sa_ap_kernel<T, 3><<<(v.nnzAP + 127) / 128, 128, 0, st>>>(v.nnzAP, v.ap_row, v.ap_cl, v.A.rowptr, v.A.col, v.A.val,
+                                                             v.p_rp, v.p_cl, v.p_val, v.ap_val);
+    pfem::count_launch();
+    sa_rap_kernel<T, 3><<<(nnzC + 127) / 128, 128, 0, st>>>(nnzC, v.c_row, v.c_cl, v.pt_rp, v.pt_blk, v.p_row, v.p_val,
+                                                           v.ap_rp, v.ap_cl, v.ap_val, cval);
+  } else {
+    pfem::count_launch();
+    sa_prolongator_kernel<T, 6><<<(v.nnzP + 127) / 128, 128, 0, st>>>(v.nnzP, v.p_row, v.p_cl, v.A.rowptr, v.A.col,
+                                                                     v.A.val, v.pslot, v.agg, v.T, v.dinv, w, v.p_val);
+    pfem::count_launch();
+    sa_ap_kernel<T, 6><<<(v.nnzAP + 127) / 128, 128, 0, st>>>(v.nnzAP, v.ap_row, v.ap_cl, v.A.rowptr, v.A.col, v.A.val,
+                                                             v.p_rp, v.p_cl, v.p_val, v.ap_val);
+    pfem::count_launch();
+    sa_rap_kernel<T, 6><<<(nnzC + 127) / 128, 128, 0, st>>>(nnzC, v.c_row, v.c_cl, v.pt_rp, v.pt_blk, v.p_row, v.p_val,
+                                                           v.ap_rp, v.ap_cl, v.ap_val, cval);
+  }
+}
+template <typename T>
+void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st) {
+  const long long n = (long long)v.nagg * 6;
+  const int blocks = (int)((n + 255) / 256);
+  pfem::count_launch();
+  if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_blk, v.p_row, v.p_val, r, bc);
+  else sa_restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_blk, v.p_row, v.p_val, r, bc);
+}
+template <typename T>
+void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
+  const long long n = (long long)v.A.nbrow * v.A.bs;
+  const int blocks = (int)((n + 255) / 256);
+  pfem::count_launch();
+  if (v.A.bs == 3) sa_prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, x);
+  else sa_prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, x);
 }
 
 // ------------------------------------------------------------------ instantiations
@@ -545,11 +671,10 @@ void dense_mv(int n, const T* M, const T* b, T* y, cudaStream_t st) {
   template void add_to_double<T>(long long, const T*, double*, cudaStream_t);                      \
   template void impose_dirichlet<T>(const BcDev&, long long, double, const double*, T*, double*,   \
                                     double*, cudaStream_t);                                        \
-  template void galerkin<T>(const BsrMat<T>&, const T*, const int*, T*, cudaStream_t);             \
-  template void amg_restrict<T>(int, int, const int*, const int*, const T*, const T*, T*,          \
-                                cudaStream_t);                                                     \
-  template void amg_prolong<T>(int, int, const int*, const T*, const T*, T*, cudaStream_t);        \
-  template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);
+  template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);                            \
+  template void sa_setup_level<T>(const AmgLevel<T>&, T, T*, int, cudaStream_t);                   \
+  template void sa_restrict<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);                    \
+  template void sa_prolong<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);
 PFEM_INST(float)
 PFEM_INST(double)
 template void convert<double, float>(long long, const double*, float*, double, cudaStream_t);

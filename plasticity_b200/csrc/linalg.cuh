@@ -41,9 +41,9 @@ template <typename A, typename B> void convert(long long n, const A* a, B* b, do
 template <typename T> void add_to_double(long long n, const T* x, double* U, cudaStream_t st);
 template <typename KT> void impose_dirichlet(const BcDev& bc, long long ndof, double lam, const double* U, KT* K, double* R, double* dg, cudaStream_t st);
 void bc_apply(const BcDev& bc, double lam, double* U, cudaStream_t st);
-template <typename T> void galerkin(const BsrMat<T>& A, const T* Tb, const int* f2c, T* cval, cudaStream_t st);
-template <typename T> void amg_restrict(int nagg, int bs, const int* aptr, const int* amem, const T* Tb, const T* r, T* bc, cudaStream_t st);
-template <typename T> void amg_prolong(int nbrow, int bs, const int* agg, const T* Tb, const T* xc, T* x, cudaStream_t st);
 template <typename T> void dense_mv(int n, const T* M, const T* b, T* y, cudaStream_t st);
+template <typename T> void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t st);
+template <typename T> void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st);
+template <typename T> void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st);
 
 }  // namespace pfem

@@ -45,20 +45,28 @@ struct BsrMat {
   VT* val = nullptr;      // device, nnzb*bs*bs (row-major blocks)
 };
 
-// One AMG level.  P is the tentative prolongator of aggregation-based AMG:
-// every fine block row n belongs to exactly one aggregate agg[n] and carries
-// a dense bs x 6 block T_n.
+// One level of smoothed-aggregation AMG.  Every fine block row n belongs to
+// one aggregate agg[n] and carries the tentative bs x 6 block T_n (the six
+// rigid-body modes, orthonormalised per aggregate).  The prolongator is
+// P = (I - w D^-1 A) T in block-CSR form (bs x 6 blocks, columns = aggregates);
+// AP is kept for the Galerkin product P^T A P that forms the next level.
 template <typename VT>
 struct AmgLevel {
   BsrMat<VT> A;
   VT* dinv = nullptr;     // nbrow x bs x bs inverse diagonal blocks
-  VT lmax = 0;            // spectral radius estimate of D^-1 A
+  VT lmax = 0;            // spectral radius estimate of D^-1 A (x 1.1)
   int nagg = 0;
   int* agg = nullptr;     // nbrow aggregate of each block row
   VT* T = nullptr;        // nbrow x bs x 6
-  int* agg_ptr = nullptr; // nagg+1 members of each aggregate (CSR)
-  int* agg_mem = nullptr;
-  int* fine2coarse = nullptr;  // per fine block: index of the coarse block it feeds
+  int nnzP = 0;
+  int *p_rp = nullptr, *p_cl = nullptr, *p_row = nullptr;  // P pattern (+ row of each block)
+  VT* p_val = nullptr;
+  int* pslot = nullptr;   // per A block: the P block of its row whose column is agg(col)
+  int *pt_rp = nullptr, *pt_blk = nullptr;  // P^T: P blocks of each aggregate
+  int nnzAP = 0;
+  int *ap_rp = nullptr, *ap_cl = nullptr, *ap_row = nullptr;
+  VT* ap_val = nullptr;
+  int *c_row = nullptr, *c_cl = nullptr;    // next level's pattern with the row of each block
   // work vectors (length nbrow*bs)
   VT *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
 };
@@ -67,6 +75,8 @@ template <typename VT>
 struct Amg {
   std::vector<AmgLevel<VT>> lv;
   int coarse_n = 0;          // dofs of the coarsest level
+  long long coarse_nnzb = 0;
+  VT* coarse_val = nullptr;  // Galerkin operator of the coarsest level (6 x 6 blocks)
   VT* coarse_inv = nullptr;  // coarse_n x coarse_n dense inverse (row-major)
   VT *cx = nullptr, *cb = nullptr;
   bool built = false;

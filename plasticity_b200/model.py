@@ -298,6 +298,15 @@ class Model:
         check(rc, self._ctx)
         return list(hist[:it.value]), list(kh[:max(it.value - 1, 0)])
 
+    def residual(self, lam, precision="fp64"):
+        """Assemble + impose at the current U (one newton! iteration's residual);
+        leaves the imposed tangent resident.  Returns (||R||, R)."""
+        self._push_bcs()
+        R = np.zeros(self.ndof)
+        rn = C.c_double()
+        check(L.lib().pfem_residual(self._ctx, float(lam), _PREC[precision], C.byref(rn), ptr(R)), self._ctx)
+        return rn.value, R
+
     def linear_solve(self, b, rtol, rebuild=True, **kw):
         o = self._opts(**kw)
         b = np.ascontiguousarray(b, np.float64)
@@ -307,6 +316,21 @@ class Model:
                                        C.byref(n))
         check(rc, self._ctx)
         return x, n.value
+
+    def amg_apply(self, r):
+        """One V-cycle of the resident AMG hierarchy: z = M^-1 r."""
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros(self.ndof)
+        check(L.lib().pfem_amg_apply(self._ctx, ptr(r), ptr(z)), self._ctx)
+        return z
+
+    def amg_dense(self, level, what):
+        """Dense copy of an AMG operator (what=0) or prolongator (what=1)."""
+        dims = np.zeros(2, np.int64)
+        check(L.lib().pfem_amg_dense(self._ctx, level, what, None, ptr(dims, L._i64)), self._ctx)
+        out = np.zeros((int(dims[0]), int(dims[1])))
+        check(L.lib().pfem_amg_dense(self._ctx, level, what, ptr(out), ptr(dims, L._i64)), self._ctx)
+        return out
 
     def reset(self):
         check(L.lib().pfem_reset(self._ctx), self._ctx)
@@ -336,6 +360,14 @@ class Model:
         U = np.zeros(self.ndof)
         check(L.lib().pfem_get_state(self._ctx, ptr(U), None, None, None, None, None), self._ctx)
         return U
+
+    def timer_start(self):
+        check(L.lib().pfem_timer(self._ctx, 0, None), self._ctx)
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        check(L.lib().pfem_timer(self._ctx, 1, C.byref(ms)), self._ctx)
+        return ms.value
 
     def profile(self, what: int, reps: int = 10) -> float:
         ms = C.c_double()

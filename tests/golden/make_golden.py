@@ -45,14 +45,25 @@ def element_cases():
 
 
 def solve_case(w, fname, line_search=False):
+    """Newton counts from a run at the case's own tolerance (the reference's
+    algorithm); U / stress / alpha / flags from a run tightened to 1e-12, which
+    is the truth the 1e-8 displacement bar is measured against."""
     mat = O.J2Material(**{k: w.material[k] for k in ("E", "nu", "sigy0", "Hiso", "Hkin")})
-    m = O.OracleModel(w.mesh.nodes, w.mesh.elements, mat, fbar=True, sigy0_e=w.sigy0_e)
-    w.apply(m)
-    res = m.solve(nsteps=w.nsteps, tol=w.tol, maxiter=25, line_search=line_search)
-    assert res["converged"]
-    np.savez_compressed(os.path.join(HERE, fname), U=m.U, tau=m.tau, alpha=m.alpha, flags=m.flags,
-                        sigma=m.gauss_stress(), iters=np.array(res["iters"]), nsteps=w.nsteps, tol=w.tol, line_search=int(line_search))
-    print(fname, res["iters"], float(np.abs(m.U).max()), float(m.alpha.max()), float(m.flags.mean()))
+    out = {}
+    for tol in (w.tol, 1e-12):
+        m = O.OracleModel(w.mesh.nodes, w.mesh.elements, mat, fbar=True, sigy0_e=w.sigy0_e)
+        w.apply(m)
+        res = m.solve(nsteps=w.nsteps, tol=tol, maxiter=25, line_search=line_search)
+        assert res["converged"]
+        if tol == w.tol:
+            out["iters"] = np.array(res["iters"])
+        else:
+            out.update(U=m.U, tau=m.tau, alpha=m.alpha, flags=m.flags, sigma=m.gauss_stress(),
+                       iters_tight=np.array(res["iters"]))
+    np.savez_compressed(os.path.join(HERE, fname), nsteps=w.nsteps, tol=w.tol,
+                        line_search=int(line_search), **out)
+    print(fname, list(out["iters"]), float(np.abs(out["U"]).max()), float(out["alpha"].max()),
+          float(out["flags"].mean()))
 
 
 if __name__ == "__main__":

@@ -94,40 +94,39 @@ def _check_solve(M, g, prec_label, iters_tol=1):
     assert np.array_equal(st["flags"], g["flags"]), prec_label
 
 
+def _solve_pair(w, g, precision):
+    """Newton counts at the case tolerance (FP64, near-exact inner solves, the
+    reference's algorithm) and the converged state at tol 1e-10."""
+    ls = bool(int(g["line_search"]))
+    if precision == "fp64":
+        M = model_from(w)
+        res = M.solve(nsteps=w.nsteps, tol=float(g["tol"]), maxiter=25, lin_rtol=1e-12, line_search=ls)
+        assert res.converged
+        assert np.abs(np.array(res.iters) - g["iters"]).max() <= 1, (res.iters, list(g["iters"]))
+    M = model_from(w)
+    res = M.solve(nsteps=w.nsteps, tol=1e-10, maxiter=25, precision=precision, line_search=ls,
+                  lin_rtol=1e-12 if precision == "fp64" else None)
+    assert res.converged
+    _check_solve(M, g, precision)
+    return res
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_config0_solve_vs_golden(precision):
     g = np.load(os.path.join(GOLD, "config0_cube8.npz"))
-    w = W.config0(n=8)
-    M = model_from(w)
-    res = M.solve(nsteps=int(g["nsteps"]), tol=float(g["tol"]), maxiter=25, precision=precision,
-                  lin_rtol=1e-12 if precision == "fp64" else 1e-6)
-    assert res.converged
-    _check_solve(M, g, precision)
-    d = np.abs(np.array(res.iters) - g["iters"])
-    assert d.max() <= 1, (res.iters, list(g["iters"]))
+    _solve_pair(W.config0(n=8), g, precision)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_jittered_compression_vs_golden(precision):
     g = np.load(os.path.join(GOLD, "cube4_jitter_compress.npz"))
-    w = W.config2(n=4, nsteps=int(g["nsteps"]))
-    M = model_from(w)
-    res = M.solve(nsteps=w.nsteps, tol=w.tol, maxiter=25, precision=precision, line_search=True,
-                  lin_rtol=1e-12 if precision == "fp64" else None)
-    assert res.converged
-    _check_solve(M, g, precision)
-    if precision == "fp64":
-        assert np.abs(np.array(res.iters) - g["iters"]).max() <= 1
+    _solve_pair(W.config2(n=4, nsteps=int(g["nsteps"])), g, precision)
 
 
-def test_necking_bar_vs_golden():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_necking_bar_vs_golden(precision):
     g = np.load(os.path.join(GOLD, "bar8x2x2_neck.npz"))
-    w = W.config1(nx=8, ny=2, nz=2, nsteps=6, stretch=0.05)
-    M = model_from(w)
-    res = M.solve(nsteps=w.nsteps, tol=w.tol, maxiter=25, lin_rtol=1e-12)
-    assert res.converged
-    _check_solve(M, g, "fp64")
-    assert np.abs(np.array(res.iters) - g["iters"]).max() <= 1
+    _solve_pair(W.config1(nx=8, ny=2, nz=2, nsteps=6, stretch=0.05), g, precision)
 
 
 def test_predictors_reach_same_solution():
@@ -147,7 +146,7 @@ def test_bicgstab_matches_cg():
     out = []
     for kry in ("cg", "bicgstab"):
         M = model_from(w)
-        res = M.solve(nsteps=3, tol=1e-10, linsolve=kry, lin_rtol=1e-12)
+        res = M.solve(nsteps=3, tol=1e-10, maxiter=40, linsolve=kry, lin_rtol=1e-9)
         assert res.converged
         out.append(M.U)
     assert rel(out[1], out[0]) < 1e-8

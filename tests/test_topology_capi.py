@@ -21,7 +21,7 @@ MAT = P.J2Material(210e3, 0.3, 250.0, 1000.0)
 
 def test_library_exports_every_header_symbol():
     hdr = open(os.path.join(ROOT, "include", "pfem_b200.h")).read()
-    names = set(re.findall(r"^\s*(?:int|void|const char\*)\s+(pfem_\w+)\s*\(", hdr, re.M))
+    names = set(re.findall(r"^\s*(?:int64_t|int|void|const char\*)\s+(pfem_\w+)\s*\(", hdr, re.M))
     assert len(names) >= 17
     lib = L.lib()
     for n in names:
