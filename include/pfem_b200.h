@@ -190,6 +190,22 @@ int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms_per_launc
  * context is launched on): op 0 records the start event; op 1 records the
  * stop event, synchronizes and returns the elapsed milliseconds in *ms. */
 int pfem_timer(pfem_ctx* ctx, int32_t op, double* ms);
+/* Euclidean norm sqrt(sum x_i^2) of a device vector, allocating nothing.  It
+ * has no counterpart in the reference.  It serves callers that cannot call
+ * cudaMalloc -- code running inside a framework that owns every device
+ * allocation through its own pool, or a caller that must keep cudaMalloc and
+ * cudaFree out of its steady state.  x (n doubles) and result (one double) are
+ * device pointers the caller owns.  The per-block partial sums live in a
+ * file-scope device array of 65,536 doubles (512 KiB on every device that
+ * loads the library, held until the process exits), so n is limited to
+ * 134,217,728 elements; a larger n returns PFEM_ERR_BAD_ARG and
+ * pfem_last_error(NULL) says why.  The call is asynchronous on `stream` (a
+ * cudaStream_t; NULL means the legacy default stream).  The first call on a
+ * device, made with that device current, looks up the scratch address; make
+ * it before any stream capture.  All calls share the scratch array, so calls
+ * that overlap on the GPU race. */
+int pfem_norm2_noalloc(const double* x, int64_t n, double* result, void* stream);
+
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t pfem_kernel_launches(void);
 

@@ -86,6 +86,7 @@ SIGNATURES = {
     "pfem_profile": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d]),
     "pfem_timer": (C.c_int, [_ctx, C.c_int32, _d]),
     "pfem_kernel_launches": (C.c_int64, []),
+    "pfem_norm2_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

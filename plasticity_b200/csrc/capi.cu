@@ -20,6 +20,7 @@ using namespace pfem;
 static thread_local std::string g_cuda_err;
 static long long g_launches = 0;
 long long& pfem::launch_counter() { return g_launches; }
+void pfem::set_last_error(const std::string& msg) { g_cuda_err = msg; }
 void pfem_set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
   char buf[512];
   snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what,

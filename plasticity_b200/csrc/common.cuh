@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <string>
 
 #define PFEM_CUDA_OK(expr)                                                        \
   do {                                                                            \
@@ -20,6 +21,8 @@ namespace pfem {
 // Process-wide count of kernel launches made by this library (every launch
 // site calls count_launch() once), read through pfem_kernel_launches().
 long long& launch_counter();
+// Set the calling thread's error message returned by pfem_last_error(NULL).
+void set_last_error(const std::string& msg);
 inline void count_launch() { ++launch_counter(); }
 
 // Material constants with the derived moduli of J2Material
