@@ -206,6 +206,31 @@ int pfem_timer(pfem_ctx* ctx, int32_t op, double* ms);
  * that overlap on the GPU race. */
 int pfem_norm2_noalloc(const double* x, int64_t n, double* result, void* stream);
 
+/* ---- Learned Newton predictor (no counterpart in the reference) ----
+ * Per-node MLP 12 -> 128 -> 128 -> 3 (GELU) on BF16 tensor cores with FP32
+ * accumulation.  Features of node n for the step to lambda_{k+1}: coordinates
+ * scaled to the bounding box minus 1/2 (3), dU_k / s and dU_{k-1} / s (3 + 3)
+ * with s = max |dU_k|, 10 x nodal-mean alpha (1), 10 x load-step size (1),
+ * lambda_{k+1} (1).  Output y: U_{k+1} = U_k + r dU_k + s y, r the step ratio
+ * (the extrapolation predictor plus a learned correction).  With predictor =
+ * PFEM_PRED_LEARNED the guess with the smaller FP64 residual (learned or
+ * extrapolated) starts Newton.  Parameters are MLP_NPARAMS = 20752 FP32 values:
+ * W1 [128][16], b1 [128], W2 [128][128], b2 [128], W3 [16][128], b3 [16]
+ * (columns 12..15 of W1 and rows 3..15 of W3 are padding, kept zero). */
+int pfem_mlp_init(pfem_ctx* ctx, uint64_t seed);
+/* op 0: copy the parameters out; op 1: load them (the predictor becomes usable). */
+int pfem_mlp_params(pfem_ctx* ctx, int32_t op, float* params, int64_t n);
+/* Forward pass on host features (n x 12) -> outputs (n x 3). */
+int pfem_mlp_forward(pfem_ctx* ctx, const float* feats, int64_t n, float* out);
+/* Mean-squared-error loss and its gradient (MLP_NPARAMS) on host data. */
+int pfem_mlp_loss_grad(pfem_ctx* ctx, const float* feats, const float* targets, int64_t n, float* grad,
+                       float* loss);
+/* Training-set recording from converged load steps: op 0 start (capacity
+ * samples), 1 stop, 2 clear; *size receives the number of recorded samples. */
+int pfem_mlp_record(pfem_ctx* ctx, int32_t op, int64_t capacity, int64_t* size);
+/* Adam (beta 0.9/0.999) on random batches of the recorded samples. */
+int pfem_mlp_train(pfem_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed, float* losses);
+
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t pfem_kernel_launches(void);
 

@@ -86,6 +86,12 @@ SIGNATURES = {
     "pfem_profile": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d]),
     "pfem_timer": (C.c_int, [_ctx, C.c_int32, _d]),
     "pfem_kernel_launches": (C.c_int64, []),
+    "pfem_mlp_init": (C.c_int, [_ctx, C.c_uint64]),
+    "pfem_mlp_params": (C.c_int, [_ctx, C.c_int32, _f, C.c_int64]),
+    "pfem_mlp_forward": (C.c_int, [_ctx, _f, C.c_int64, _f]),
+    "pfem_mlp_loss_grad": (C.c_int, [_ctx, _f, _f, C.c_int64, _f, _f]),
+    "pfem_mlp_record": (C.c_int, [_ctx, C.c_int32, C.c_int64, _i64]),
+    "pfem_mlp_train": (C.c_int, [_ctx, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _f]),
     "pfem_norm2_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
 }
 

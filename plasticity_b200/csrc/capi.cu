@@ -83,6 +83,8 @@ struct pfem_ctx {
   double *dCpi = nullptr, *dAlpha = nullptr, *dEpsp = nullptr, *dTau = nullptr;
   uint8_t* dFlags = nullptr;
   double *dU = nullptr, *dR = nullptr, *dDg = nullptr, *dUprev = nullptr, *dUprev2 = nullptr;
+  double* dUprev3 = nullptr;
+  double bbox_lo[3] = {0, 0, 0}, bbox_ext[3] = {1, 1, 1};
   double *dUtmp = nullptr, *dScal = nullptr, *dPart = nullptr;
   double* dK64 = nullptr;
   float* dK32 = nullptr;
@@ -948,13 +950,13 @@ struct StepTimes {
 // assembly becomes the next iterate, so line search costs extra assemblies
 // only when it backtracks.
 int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, double* hist,
-               int* khist, bool* converged, StepTimes* tm) {
+               int* khist, bool* converged, StepTimes* tm, bool have_first = false, double rn_first = 0.0) {
   *converged = false;
   const double fext_norm = std::fabs(lam) * ctx->fn_norm;
   double ref = 1.0, rkm1 = 0.0, eta_prev = o->eta_max;
-  bool first = true;
-  double rn = 0;
-  int rc = residual_system(ctx, o->precision, lam, &rn, &tm->asm_ms);
+  bool first = true, damped = false;
+  double rn = rn_first;
+  int rc = have_first ? PFEM_OK : residual_system(ctx, o->precision, lam, &rn, &tm->asm_ms);
   if (rc) return rc;
   int it;
   for (it = 1; it <= o->maxiter; ++it) {
@@ -968,6 +970,9 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     }
     if (it == o->maxiter) break;
     double eta = o->lin_rtol > 0 ? o->lin_rtol : forcing_term(o, it, rn, rkm1, eta_prev);
+    // After a backtracked step the iterate is outside Newton's fast region; a
+    // loose inner solve there gives poor directions, so tighten it.
+    if (damped) eta = std::min(eta, 1e-3);
     const bool rebuild = first || o->amg_rebuild;
     first = false;
     int kits = 0;
@@ -997,6 +1002,8 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
       if (bt >= 8) return rc ? rc : fail(ctx, PFEM_ERR_NOT_CONVERGED, "line search failed");
       a *= 0.5;
     }
+    if (o->verbose) fprintf(stderr, "      eta %.2e  krylov %d  step %.4g\n", eta, kits, a);
+    damped = a < 1.0;
     rn = rt;
   }
   *iters = std::min(it, o->maxiter);
@@ -1208,6 +1215,12 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     for (int64_t e = 0; e < ne; ++e) clist[f[col[e]]++] = (int)e;
   }
   std::iota(all.begin(), all.end(), 0);
+  for (int d = 0; d < 3; ++d) {
+    double lo = 1e300, hi = -1e300;
+    for (int64_t n = 0; n < nn; ++n) { lo = std::min(lo, ctx->X[n * 3 + d]); hi = std::max(hi, ctx->X[n * 3 + d]); }
+    ctx->bbox_lo[d] = lo;
+    ctx->bbox_ext[d] = hi > lo ? hi - lo : 1.0;
+  }
   if (device < 0) {  // topology-only context: pattern / colors, no device work
     *out = ctx;
     return PFEM_OK;
@@ -1237,6 +1250,7 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
   AL(ctx->dDg, ctx->ndof);
   AL(ctx->dUprev, ctx->ndof);
   AL(ctx->dUprev2, ctx->ndof);
+  AL(ctx->dUprev3, ctx->ndof);
   AL(ctx->dUtmp, ctx->ndof);
   AL(ctx->dScal, 16);
   AL(ctx->dPart, 2048);
@@ -1258,7 +1272,6 @@ void pfem_destroy(pfem_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   for (void* p : ctx->allocs) cudaFree(p);
-  pfem::mlp_free(ctx->mlp);
   if (ctx->e0) cudaEventDestroy(ctx->e0);
   if (ctx->e1) cudaEventDestroy(ctx->e1);
   if (ctx->t0) cudaEventDestroy(ctx->t0);
@@ -1415,8 +1428,11 @@ int pfem_reset(pfem_ctx* ctx) {
   CK(cudaMemsetAsync(ctx->dU, 0, ctx->ndof * sizeof(double), ctx->st));
   CK(cudaMemsetAsync(ctx->dUprev, 0, ctx->ndof * sizeof(double), ctx->st));
   CK(cudaMemsetAsync(ctx->dUprev2, 0, ctx->ndof * sizeof(double), ctx->st));
+  CK(cudaMemsetAsync(ctx->dUprev3, 0, ctx->ndof * sizeof(double), ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   ctx->steps_taken = 0;
+  ctx->mlp.used_count = 0;
+  ctx->mlp.have_feat = false;
   ctx->lam_prev = ctx->lam_prev2 = 0.0;
   return PFEM_OK;
 }
@@ -1490,16 +1506,92 @@ int pfem_assemble(pfem_ctx* ctx, const double* U, int32_t commit, int32_t precis
   return pfem_get_state(ctx, nullptr, tau, nullptr, nullptr, nullptr, flags);
 }
 
-static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepTimes* tm) {
-  // predictor for this load step (previous U is the reference's choice)
+static int mlp_alloc(pfem_ctx* ctx) {
+  MlpState& m = ctx->mlp;
+  if (m.alloc) return PFEM_OK;
+  CK(dalloc(ctx, &m.w, MLP_NPARAMS)); CK(dalloc(ctx, &m.m, MLP_NPARAMS)); CK(dalloc(ctx, &m.v, MLP_NPARAMS));
+  CK(dalloc(ctx, &m.g, MLP_NPARAMS)); CK(dalloc(ctx, &m.loss, 4)); CK(dalloc(ctx, &m.err, 4));
+  char* f = nullptr;
+  CK(dalloc(ctx, &f, (size_t)ctx->nn * 32));
+  m.feat = f;
+  CK(dalloc(ctx, &m.out, (size_t)ctx->nn * 3));
+  CK(dalloc(ctx, &m.anode, (size_t)ctx->nn));
+  CK(dalloc(ctx, &m.scale, 4));
+  std::vector<float> val(ctx->nn, 0.0f);
+  for (long long e = 0; e < ctx->ne; ++e)
+    for (int a = 0; a < 8; ++a) val[ctx->elem[e * 8 + a]] += 1.0f;
+  CK(upload(ctx, &m.valence, val));
+  CK(cudaMemset(m.m, 0, MLP_NPARAMS * sizeof(float)));
+  CK(cudaMemset(m.v, 0, MLP_NPARAMS * sizeof(float)));
+  CK(cudaMemset(m.w, 0, MLP_NPARAMS * sizeof(float)));
+  CK(cudaMemset(m.err, 0, 4 * sizeof(int)));
+  m.alloc = true;
+  return PFEM_OK;
+}
+
+static int mlp_check_err(pfem_ctx* ctx) {
+  int e = 0;
+  CK(cudaMemcpy(&e, ctx->mlp.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(ctx->mlp.err, 0, sizeof(int));
+    return fail(ctx, PFEM_ERR_CUDA, "tensor-core MMA wait timed out in the predictor kernel");
+  }
+  return PFEM_OK;
+}
+
+// Predictor for the load step to lambda.  Returns, when the learned guess was
+// evaluated, the FP64 residual of the guess that was kept (its tangent is
+// resident), so Newton can start from it without re-assembling.
+static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepTimes* tm, bool* have_first,
+                      double* rn_first) {
   const long long n = ctx->ndof;
+  *have_first = false;
   auto t0 = std::chrono::steady_clock::now();
+  MlpState& ml = ctx->mlp;
+  ml.have_feat = false;
+  const double dl_prev = ctx->lam_prev - ctx->lam_prev2;
+  const double r = dl_prev > 0 ? (lam - ctx->lam_prev) / dl_prev : 0.0;
   if (o->predictor != PFEM_PRED_PREVIOUS && ctx->steps_taken >= 1) {
-    const double dl = ctx->lam_prev - ctx->lam_prev2;
-    const double f = dl > 0 ? (lam - ctx->lam_prev) / dl : 0.0;
-    pfem::count_launch(); extrap_kernel<<<1024, 256, 0, ctx->st>>>(n, f, ctx->dUprev, ctx->dUprev2, ctx->dU);
+    pfem::count_launch(); extrap_kernel<<<1024, 256, 0, ctx->st>>>(n, r, ctx->dUprev, ctx->dUprev2, ctx->dU);
     bc_apply(ctx->bc, lam, ctx->dU, ctx->st);
     CKL();
+  }
+  const bool want_learned = o->predictor == PFEM_PRED_LEARNED && ml.ready;
+  if ((ml.recording || want_learned) && ctx->steps_taken >= 2 && o->predictor != PFEM_PRED_PREVIOUS) {
+    int rc = mlp_alloc(ctx);
+    if (rc) return rc;
+    mlp_nodal_alpha(ctx->ne, ctx->nn, ctx->dElem, ctx->dAlpha, ml.valence, ml.anode, ctx->st);
+    mlp_features(ctx->nn, ctx->dX, ctx->bbox_lo, ctx->bbox_ext, ctx->dUprev, ctx->dUprev2, ctx->dUprev3, ml.anode,
+                 lam - ctx->lam_prev, lam, ml.scale, ctx->dPart, ml.feat, ctx->st);
+    CKL();
+    ml.have_feat = true;
+    ml.r_ratio = r;
+  }
+  if (want_learned && ml.have_feat) {
+    // FP64 residual of the extrapolated guess, then of the learned one; keep the smaller.
+    double r_ex = 0, r_ml = 0;
+    int rc = residual_system(ctx, o->precision, lam, &r_ex, &tm->asm_ms);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->dUtmp, ctx->dU, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+    rc = mlp_launch(false, ml.w, ml.feat, nullptr, nullptr, ctx->nn, ml.out, nullptr, nullptr, ml.err, 148, ctx->st);
+    if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
+    mlp_apply(ctx->nn, ctx->dUprev, ctx->dUprev2, r, ml.scale, ml.out, ctx->dU, ctx->st);
+    bc_apply(ctx->bc, lam, ctx->dU, ctx->st);
+    CKL();
+    rc = mlp_check_err(ctx);
+    if (rc) return rc;
+    rc = residual_system(ctx, o->precision, lam, &r_ml, &tm->asm_ms);
+    const bool learned_ok = rc == PFEM_OK && std::isfinite(r_ml) && r_ml < r_ex;
+    if (rc && rc != PFEM_ERR_INVERTED_ELEMENT) return rc;
+    if (learned_ok) {
+      ml.used_count++;
+      *rn_first = r_ml;
+    } else {
+      CK(cudaMemcpyAsync(ctx->dU, ctx->dUtmp, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+      rc = residual_system(ctx, o->precision, lam, rn_first, &tm->asm_ms);
+      if (rc) return rc;
+    }
+    *have_first = true;
   }
   CK(cudaStreamSynchronize(ctx->st));
   tm->pred_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1507,6 +1599,17 @@ static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepT
 }
 
 static int step_end(pfem_ctx* ctx, double lam) {
+  MlpState& ml = ctx->mlp;
+  if (ml.recording && ml.have_feat && ml.ds_n + ctx->nn <= ml.ds_cap) {
+    // training pair: features of this step, target = (dU_{n+1} - r dU_n) / s
+    CK(cudaMemcpyAsync(static_cast<char*>(ml.ds_x) + (size_t)ml.ds_n * 32, ml.feat, (size_t)ctx->nn * 32,
+                       cudaMemcpyDeviceToDevice, ctx->st));
+    mlp_targets(ctx->nn, ctx->dU, ctx->dUprev, ctx->dUprev2, ml.r_ratio, ml.scale, ml.ds_t + (size_t)ml.ds_n * 3,
+                ctx->st);
+    CKL();
+    ml.ds_n += ctx->nn;
+  }
+  CK(cudaMemcpyAsync(ctx->dUprev3, ctx->dUprev2, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
   CK(cudaMemcpyAsync(ctx->dUprev2, ctx->dUprev, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
   CK(cudaMemcpyAsync(ctx->dUprev, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
   ctx->lam_prev2 = ctx->lam_prev;
@@ -1522,12 +1625,14 @@ int pfem_newton(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, int32_t*
   if (!ctx->bcs_set) return fail(ctx, PFEM_ERR_STATE, "pfem_set_bcs must be called first");
   cudaSetDevice(ctx->device);
   StepTimes tm;
-  int rc = step_begin(ctx, lambda, o, &tm);
+  bool hf = false;
+  double r0 = 0;
+  int rc = step_begin(ctx, lambda, o, &tm, &hf, &r0);
   if (rc) return rc;
   std::vector<int> kh(o->maxiter, 0);
   bool conv = false;
   int it = 0;
-  rc = newton_dev(ctx, lambda, o, &it, res_hist, kh.data(), &conv, &tm);
+  rc = newton_dev(ctx, lambda, o, &it, res_hist, kh.data(), &conv, &tm, hf, r0);
   if (iters) *iters = it;
   if (krylov_hist) std::copy(kh.begin(), kh.end(), krylov_hist);
   if (rc) return rc;
@@ -1553,12 +1658,14 @@ int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res, 
   for (int n = 1; n <= o->nsteps; ++n) {
     const double lam = (double)n / o->nsteps;
     if (o->verbose) fprintf(stderr, "Load step %d/%d  (lambda=%g)\n", n, o->nsteps, lam);
-    rc = step_begin(ctx, lam, o, &tm);
+    bool hf = false;
+    double r0 = 0;
+    rc = step_begin(ctx, lam, o, &tm, &hf, &r0);
     if (rc) return rc;
     bool conv = false;
     int it = 0;
     rc = newton_dev(ctx, lam, o, &it, residuals ? residuals + (size_t)(n - 1) * o->maxiter : nullptr,
-                    krylov_per_iter ? krylov_per_iter + (size_t)(n - 1) * o->maxiter : nullptr, &conv, &tm);
+                    krylov_per_iter ? krylov_per_iter + (size_t)(n - 1) * o->maxiter : nullptr, &conv, &tm, hf, r0);
     if (rc) return rc;
     if (iters_per_step) iters_per_step[n - 1] = it;
     r.newton_iters_total += it;
@@ -1780,6 +1887,160 @@ int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms) {
 }
 
 int64_t pfem_kernel_launches(void) { return (int64_t)g_launches; }
+
+int pfem_mlp_init(pfem_ctx* ctx, uint64_t seed) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc = mlp_alloc(ctx);
+  if (rc) return rc;
+  // He-uniform weights (fan-in of the real inputs), zero biases; padding stays zero.
+  std::vector<float> p(MLP_NPARAMS, 0.0f);
+  uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto uni = [&]() {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return (double)((st >> 11) & ((1ull << 53) - 1)) / (double)(1ull << 53) * 2.0 - 1.0;
+  };
+  const int H = 128;
+  for (int h = 0; h < H; ++h)
+    for (int i = 0; i < MLP_NFEAT; ++i) p[h * 16 + i] = (float)(uni() * std::sqrt(6.0 / MLP_NFEAT));
+  const int oW2 = H * 16 + H;
+  for (int i = 0; i < H * H; ++i) p[oW2 + i] = (float)(uni() * std::sqrt(6.0 / H));
+  const int oW3 = oW2 + H * H + H;
+  for (int o = 0; o < 3; ++o)
+    for (int h = 0; h < H; ++h) p[oW3 + o * H + h] = (float)(uni() * std::sqrt(6.0 / H) * 0.1);
+  CK(cudaMemcpy(ctx->mlp.w, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemset(ctx->mlp.m, 0, MLP_NPARAMS * sizeof(float)));
+  CK(cudaMemset(ctx->mlp.v, 0, MLP_NPARAMS * sizeof(float)));
+  ctx->mlp.adam_t = 0;
+  ctx->mlp.ready = false;
+  return PFEM_OK;
+}
+
+int pfem_mlp_params(pfem_ctx* ctx, int32_t op, float* p, int64_t n) {
+  if (!ctx || !p || n != MLP_NPARAMS) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc = mlp_alloc(ctx);
+  if (rc) return rc;
+  if (op == 0) {
+    CK(cudaMemcpy(p, ctx->mlp.w, MLP_NPARAMS * sizeof(float), cudaMemcpyDeviceToHost));
+  } else {
+    CK(cudaMemcpy(ctx->mlp.w, p, MLP_NPARAMS * sizeof(float), cudaMemcpyHostToDevice));
+    ctx->mlp.ready = true;
+  }
+  return PFEM_OK;
+}
+
+int pfem_mlp_forward(pfem_ctx* ctx, const float* feats, int64_t n, float* out) {
+  if (!ctx || !feats || !out || n <= 0) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc = mlp_alloc(ctx);
+  if (rc) return rc;
+  float *df = nullptr, *dy = nullptr;
+  void* db = nullptr;
+  CK(cudaMalloc((void**)&df, (size_t)n * MLP_NFEAT * sizeof(float)));
+  CK(cudaMalloc(&db, (size_t)n * 32));
+  CK(cudaMalloc((void**)&dy, (size_t)n * 3 * sizeof(float)));
+  CK(cudaMemcpy(df, feats, (size_t)n * MLP_NFEAT * sizeof(float), cudaMemcpyHostToDevice));
+  mlp_pack_features(df, n, db, ctx->st);
+  rc = mlp_launch(false, ctx->mlp.w, db, nullptr, nullptr, n, dy, nullptr, nullptr, ctx->mlp.err, 148, ctx->st);
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaMemcpy(out, dy, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaFree(df); cudaFree(db); cudaFree(dy);
+  if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
+  return mlp_check_err(ctx);
+}
+
+int pfem_mlp_loss_grad(pfem_ctx* ctx, const float* feats, const float* targets, int64_t n, float* grad, float* loss) {
+  if (!ctx || !feats || !targets || n <= 0) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc = mlp_alloc(ctx);
+  if (rc) return rc;
+  float *df = nullptr, *dt = nullptr;
+  void* db = nullptr;
+  CK(cudaMalloc((void**)&df, (size_t)n * MLP_NFEAT * sizeof(float)));
+  CK(cudaMalloc(&db, (size_t)n * 32));
+  CK(cudaMalloc((void**)&dt, (size_t)n * 3 * sizeof(float)));
+  CK(cudaMemcpy(df, feats, (size_t)n * MLP_NFEAT * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dt, targets, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice));
+  mlp_pack_features(df, n, db, ctx->st);
+  CK(cudaMemsetAsync(ctx->mlp.g, 0, MLP_NPARAMS * sizeof(float), ctx->st));
+  CK(cudaMemsetAsync(ctx->mlp.loss, 0, sizeof(float), ctx->st));
+  rc = mlp_launch(true, ctx->mlp.w, db, dt, nullptr, n, nullptr, ctx->mlp.g, ctx->mlp.loss, ctx->mlp.err, 148,
+                  ctx->st);
+  CK(cudaStreamSynchronize(ctx->st));
+  if (grad) CK(cudaMemcpy(grad, ctx->mlp.g, MLP_NPARAMS * sizeof(float), cudaMemcpyDeviceToHost));
+  float l = 0;
+  CK(cudaMemcpy(&l, ctx->mlp.loss, sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) *loss = l / (3.0f * (float)n);
+  cudaFree(df); cudaFree(db); cudaFree(dt);
+  if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
+  return mlp_check_err(ctx);
+}
+
+int pfem_mlp_record(pfem_ctx* ctx, int32_t op, int64_t capacity, int64_t* size) {
+  if (!ctx) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  int rc = mlp_alloc(ctx);
+  if (rc) return rc;
+  MlpState& m = ctx->mlp;
+  if (op == 0) {
+    if (capacity > m.ds_cap) {
+      if (m.ds_x) { cudaFree(m.ds_x); cudaFree(m.ds_t); }
+      m.ds_x = nullptr; m.ds_t = nullptr;
+      CK(cudaMalloc(&m.ds_x, (size_t)capacity * 32));
+      CK(cudaMalloc((void**)&m.ds_t, (size_t)capacity * 3 * sizeof(float)));
+      m.ds_cap = capacity;
+    }
+    m.recording = true;
+  } else if (op == 1) {
+    m.recording = false;
+  } else if (op == 2) {
+    m.ds_n = 0;
+  }
+  if (size) *size = m.ds_n;
+  return PFEM_OK;
+}
+
+int pfem_mlp_train(pfem_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed, float* losses) {
+  if (!ctx || steps <= 0 || batch <= 0) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  cudaSetDevice(ctx->device);
+  MlpState& m = ctx->mlp;
+  if (!m.alloc || m.ds_n <= 0) return fail(ctx, PFEM_ERR_STATE, "no recorded training samples");
+  if (batch > m.rows_cap) {
+    int* r = nullptr;
+    CK(dalloc(ctx, &r, (size_t)batch));
+    m.rows = r;
+    m.rows_cap = batch;
+  }
+  float* dl = nullptr;
+  CK(cudaMalloc((void**)&dl, (size_t)steps * sizeof(float)));
+  int rc = 0;
+  for (int k = 0; k < steps; ++k) {
+    mlp_random_rows(batch, m.ds_n, seed * 1000003ull + (uint64_t)k, m.rows, ctx->st);
+    CK(cudaMemsetAsync(m.g, 0, MLP_NPARAMS * sizeof(float), ctx->st));
+    CK(cudaMemsetAsync(dl + k, 0, sizeof(float), ctx->st));
+    rc |= mlp_launch(true, m.w, m.ds_x, m.ds_t, m.rows, batch, nullptr, m.g, dl + k, m.err, 148, ctx->st);
+    mlp_adam(m.w, m.m, m.v, m.g, lr, ++m.adam_t, ctx->st);
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  if (losses) {
+    std::vector<float> h(steps);
+    CK(cudaMemcpy(h.data(), dl, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < steps; ++k) losses[k] = h[k] / (3.0f * (float)batch);
+  }
+  cudaFree(dl);
+  if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor training kernel launch failed");
+  rc = mlp_check_err(ctx);
+  if (rc) return rc;
+  m.ready = true;
+  return PFEM_OK;
+}
 
 int pfem_timer(pfem_ctx* ctx, int32_t op, double* ms) {
   if (!ctx) return PFEM_ERR_BAD_ARG;

@@ -369,6 +369,49 @@ class Model:
         check(L.lib().pfem_timer(self._ctx, 1, C.byref(ms)), self._ctx)
         return ms.value
 
+    # --- learned predictor (no counterpart in the reference) ---
+    NPARAMS = 20752
+
+    def mlp_init(self, seed=0):
+        check(L.lib().pfem_mlp_init(self._ctx, int(seed)), self._ctx)
+
+    def mlp_params(self, params=None):
+        """Return the FP32 parameter vector, or load `params` (marks the predictor usable)."""
+        if params is None:
+            p = np.zeros(self.NPARAMS, np.float32)
+            check(L.lib().pfem_mlp_params(self._ctx, 0, ptr(p, L._f), self.NPARAMS), self._ctx)
+            return p
+        p = np.ascontiguousarray(params, np.float32)
+        check(L.lib().pfem_mlp_params(self._ctx, 1, ptr(p, L._f), self.NPARAMS), self._ctx)
+        return p
+
+    def mlp_forward(self, feats):
+        f = np.ascontiguousarray(feats, np.float32)
+        y = np.zeros((f.shape[0], 3), np.float32)
+        check(L.lib().pfem_mlp_forward(self._ctx, ptr(f, L._f), f.shape[0], ptr(y, L._f)), self._ctx)
+        return y
+
+    def mlp_loss_grad(self, feats, targets):
+        f = np.ascontiguousarray(feats, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        g = np.zeros(self.NPARAMS, np.float32)
+        l = C.c_float()
+        check(L.lib().pfem_mlp_loss_grad(self._ctx, ptr(f, L._f), ptr(t, L._f), f.shape[0], ptr(g, L._f),
+                                         C.byref(l)), self._ctx)
+        return l.value, g
+
+    def mlp_record(self, op, capacity=0):
+        n = C.c_int64()
+        check(L.lib().pfem_mlp_record(self._ctx, {"start": 0, "stop": 1, "clear": 2, "size": 3}[op],
+                                      int(capacity), C.byref(n)), self._ctx)
+        return n.value
+
+    def mlp_train(self, steps, batch=65536, lr=1e-3, seed=0):
+        losses = np.zeros(steps, np.float32)
+        check(L.lib().pfem_mlp_train(self._ctx, int(steps), int(batch), float(lr), int(seed), ptr(losses, L._f)),
+              self._ctx)
+        return losses
+
     def profile(self, what: int, reps: int = 10) -> float:
         ms = C.c_double()
         check(L.lib().pfem_profile(self._ctx, what, reps, C.byref(ms)), self._ctx)
