@@ -77,6 +77,9 @@ typedef struct pfem_solve_opts {
                             most 8 times) until the FP64 residual norm decreases -- the
                             accepted trial assembly is the next iterate, so a full step
                             costs nothing extra */
+  int32_t predictor_smooth; /* learned predictor only: degree of the block-Jacobi Chebyshev
+                            smoothing applied to the network's correction, on the tangent
+                            at the extrapolated guess (0 = none) */
 } pfem_solve_opts;
 
 typedef struct pfem_solve_result {
@@ -139,6 +142,18 @@ int pfem_assemble(pfem_ctx* ctx, const double* U, int32_t commit, int32_t precis
  * maxiter) receive the residual norms and Krylov iteration counts. */
 int pfem_newton(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, int32_t* iters,
                 double* res_hist, int32_t* krylov_hist);
+
+/* The Newton predictor alone for the load step to lambda (no counterpart in
+ * the reference, whose predictor is the previous converged U, Solver.jl:321-323):
+ * o->predictor selects extrapolation or the learned guess; the chosen guess is
+ * left in the context's U (copied to U, ndof, when non-null), so a following
+ * pfem_newton with predictor PFEM_PRED_PREVIOUS starts from it.  r_extrap /
+ * r_learned receive the imposed FP64 residual norms of the two guesses
+ * (r_learned = -1 when the learned guess was not evaluated: no trained
+ * weights, or fewer than two converged steps); learned_used = 1 when the
+ * learned guess was kept. */
+int pfem_predict(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, double* U, double* r_extrap,
+                 double* r_learned, int32_t* learned_used);
 
 /* solve! (Solver.jl:419-475): reset, load loop, Newton, commit.
  * iters_per_step (nsteps), residuals (nsteps x maxiter, row per step) and
@@ -208,13 +223,18 @@ int pfem_norm2_noalloc(const double* x, int64_t n, double* result, void* stream)
 
 /* ---- Learned Newton predictor (no counterpart in the reference) ----
  * Per-node MLP 12 -> 128 -> 128 -> 3 (GELU) on BF16 tensor cores with FP32
- * accumulation.  Features of node n for the step to lambda_{k+1}: coordinates
- * scaled to the bounding box minus 1/2 (3), dU_k / s and dU_{k-1} / s (3 + 3)
- * with s = max |dU_k|, 10 x nodal-mean alpha (1), 10 x load-step size (1),
- * lambda_{k+1} (1).  Output y: U_{k+1} = U_k + r dU_k + s y, r the step ratio
- * (the extrapolation predictor plus a learned correction).  With predictor =
- * PFEM_PRED_LEARNED the guess with the smaller FP64 residual (learned or
- * extrapolated) starts Newton.  Parameters are MLP_NPARAMS = 20752 FP32 values:
+ * accumulation.  Features of node n for the step to lambda_{k+1}, from the two
+ * previous converged increments dU_k and dU_{k-1}: coordinates scaled to the
+ * bounding box minus 1/2 (3), dU_k / s1 (3) with s1 = max |dU_k|, the second
+ * difference d2 = dU_k - rho dU_{k-1} over s2 = max |d2| (3; rho the ratio of
+ * the two previous load-step sizes), 10 x nodal-mean alpha (1), 10 x
+ * load-step size (1), lambda_{k+1} (1).  Output y: U_{k+1} = U_k + r dU_k +
+ * s2 y, r the step ratio -- the extrapolation predictor plus a learned
+ * correction measured in units of the second difference, so BF16 resolution
+ * applies to the correction itself.  With predictor = PFEM_PRED_LEARNED the
+ * network's correction is smoothed (pfem_solve_opts.predictor_smooth) and the
+ * guess with the smaller FP64 residual (learned or extrapolated) starts
+ * Newton.  Parameters are MLP_NPARAMS = 20752 FP32 values:
  * W1 [128][16], b1 [128], W2 [128][128], b2 [128], W3 [16][128], b3 [16]
  * (columns 12..15 of W1 and rows 3..15 of W3 are padding, kept zero). */
 int pfem_mlp_init(pfem_ctx* ctx, uint64_t seed);

@@ -42,7 +42,7 @@ class SolveOpts(C.Structure):
                 ("eta_min", C.c_double), ("eta_max", C.c_double), ("ew_gamma", C.c_double),
                 ("ew_alpha", C.c_double), ("krylov_itmax", C.c_int32), ("predictor", C.c_int32),
                 ("amg_rebuild", C.c_int32), ("cheb_degree", C.c_int32), ("verbose", C.c_int32),
-                ("line_search", C.c_int32)]
+                ("line_search", C.c_int32), ("predictor_smooth", C.c_int32)]
 
 
 class SolveResultC(C.Structure):
@@ -76,6 +76,7 @@ SIGNATURES = {
     "pfem_newton": (C.c_int, [_ctx, C.c_double, C.POINTER(SolveOpts), _i32, _d, _i32]),
     "pfem_solve": (C.c_int, [_ctx, C.POINTER(SolveOpts), C.POINTER(SolveResultC), _i32, _d, _i32]),
     "pfem_residual": (C.c_int, [_ctx, C.c_double, C.c_int32, _d, _d]),
+    "pfem_predict": (C.c_int, [_ctx, C.c_double, C.POINTER(SolveOpts), _d, _d, _d, _i32]),
     "pfem_linear_solve": (C.c_int, [_ctx, _d, _d, C.c_double, C.c_int32, C.POINTER(SolveOpts), _i32]),
     "pfem_amg_apply": (C.c_int, [_ctx, _d, _d]),
     "pfem_amg_dense": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d, _i64]),

@@ -105,7 +105,7 @@ struct pfem_ctx {
   // learned predictor
   pfem::MlpState mlp;
   int steps_taken = 0;
-  double lam_prev = 0.0, lam_prev2 = 0.0;
+  double lam_prev = 0.0, lam_prev2 = 0.0, lam_prev3 = 0.0;
 };
 
 namespace {
@@ -1036,6 +1036,38 @@ __global__ void init_state_kernel(long long ngp, double* cpi, double* alpha, dou
 }  // namespace
 
 template <typename T>
+__global__ void diff_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
+                            T* __restrict__ x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = (T)(a[i] - b[i]);
+}
+
+// Smooth the learned correction Delta = U - Utmp (U the network's guess, Utmp
+// the extrapolated one, whose imposed tangent K and residual R are resident)
+// with `degree` block-Jacobi Chebyshev steps on K Delta = -R over
+// [lmax/30, lmax]: the network's node-to-node scatter is high-frequency,
+// exactly what the smoother removes, while the smooth part of its correction
+// is kept.  lmax is the previous load step's estimate on the finest level.
+template <typename T>
+static int smooth_prediction(pfem_ctx* ctx, double lam, int degree) {
+  Amg<T>& A = amg_of<T>(ctx);
+  if (!A.built || degree <= 0) return PFEM_OK;
+  KrylovWork<T>& w = kw_of<T>(ctx);
+  AmgLevel<T>& v = A.lv[0];
+  v.A.val = K_of<T>(ctx);
+  blockdiag_invert<T>(v.A, v.dinv, ctx->st);
+  convert<double, T>(ctx->ndof, ctx->dR, w.b, -1.0, ctx->st);
+  pfem::count_launch();
+  diff_kernel<T><<<1024, 256, 0, ctx->st>>>(ctx->ndof, ctx->dU, ctx->dUtmp, w.x);
+  cheb<T>(ctx, v, degree, w.b, w.x, false);
+  pfem::count_launch();
+  step_kernel<T><<<1024, 256, 0, ctx->st>>>(ctx->ndof, 1.0, w.x, ctx->dUtmp, ctx->dU);
+  bc_apply(ctx->bc, lam, ctx->dU, ctx->st);
+  CKL();
+  return PFEM_OK;
+}
+
+template <typename T>
 static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t* dims) {
   Amg<T>& A = amg_of<T>(ctx);
   const int L = (int)A.lv.size();
@@ -1092,6 +1124,7 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->cheb_degree = 2;
   o->verbose = 0;
   o->line_search = 0;
+  o->predictor_smooth = 4;
 }
 
 const char* pfem_last_error(const pfem_ctx* ctx) {
@@ -1433,7 +1466,7 @@ int pfem_reset(pfem_ctx* ctx) {
   ctx->steps_taken = 0;
   ctx->mlp.used_count = 0;
   ctx->mlp.have_feat = false;
-  ctx->lam_prev = ctx->lam_prev2 = 0.0;
+  ctx->lam_prev = ctx->lam_prev2 = ctx->lam_prev3 = 0.0;
   return PFEM_OK;
 }
 
@@ -1549,8 +1582,12 @@ static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepT
   auto t0 = std::chrono::steady_clock::now();
   MlpState& ml = ctx->mlp;
   ml.have_feat = false;
+  ml.last_r_ex = ml.last_r_ml = -1.0;
+  ml.last_used = false;
   const double dl_prev = ctx->lam_prev - ctx->lam_prev2;
   const double r = dl_prev > 0 ? (lam - ctx->lam_prev) / dl_prev : 0.0;
+  const double dl_prev2 = ctx->lam_prev2 - ctx->lam_prev3;
+  const double rho = dl_prev2 > 0 ? dl_prev / dl_prev2 : 0.0;  // dU_n ~ rho dU_{n-1} when linear
   if (o->predictor != PFEM_PRED_PREVIOUS && ctx->steps_taken >= 1) {
     pfem::count_launch(); extrap_kernel<<<1024, 256, 0, ctx->st>>>(n, r, ctx->dUprev, ctx->dUprev2, ctx->dU);
     bc_apply(ctx->bc, lam, ctx->dU, ctx->st);
@@ -1562,7 +1599,7 @@ static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepT
     if (rc) return rc;
     mlp_nodal_alpha(ctx->ne, ctx->nn, ctx->dElem, ctx->dAlpha, ml.valence, ml.anode, ctx->st);
     mlp_features(ctx->nn, ctx->dX, ctx->bbox_lo, ctx->bbox_ext, ctx->dUprev, ctx->dUprev2, ctx->dUprev3, ml.anode,
-                 lam - ctx->lam_prev, lam, ml.scale, ctx->dPart, ml.feat, ctx->st);
+                 lam - ctx->lam_prev, lam, rho, ml.scale, ctx->dPart, ml.feat, ctx->st);
     CKL();
     ml.have_feat = true;
     ml.r_ratio = r;
@@ -1580,9 +1617,16 @@ static int step_begin(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, StepT
     CKL();
     rc = mlp_check_err(ctx);
     if (rc) return rc;
+    rc = o->precision == PFEM_FP64 ? smooth_prediction<double>(ctx, lam, o->predictor_smooth)
+                                   : smooth_prediction<float>(ctx, lam, o->predictor_smooth);
+    if (rc) return rc;
     rc = residual_system(ctx, o->precision, lam, &r_ml, &tm->asm_ms);
+    if (o->verbose) fprintf(stderr, "  predictor: |R| extrapolated %.6e  learned %.6e\n", r_ex, r_ml);
     const bool learned_ok = rc == PFEM_OK && std::isfinite(r_ml) && r_ml < r_ex;
     if (rc && rc != PFEM_ERR_INVERTED_ELEMENT) return rc;
+    ml.last_r_ex = r_ex;
+    ml.last_r_ml = r_ml;
+    ml.last_used = learned_ok;
     if (learned_ok) {
       ml.used_count++;
       *rn_first = r_ml;
@@ -1612,6 +1656,7 @@ static int step_end(pfem_ctx* ctx, double lam) {
   CK(cudaMemcpyAsync(ctx->dUprev3, ctx->dUprev2, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
   CK(cudaMemcpyAsync(ctx->dUprev2, ctx->dUprev, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
   CK(cudaMemcpyAsync(ctx->dUprev, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+  ctx->lam_prev3 = ctx->lam_prev2;
   ctx->lam_prev2 = ctx->lam_prev;
   ctx->lam_prev = lam;
   ctx->steps_taken++;
@@ -1640,6 +1685,29 @@ int pfem_newton(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, int32_t*
   rc = commit_dev(ctx);
   if (rc) return rc;
   return step_end(ctx, lambda);
+}
+
+int pfem_predict(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, double* U, double* r_extrap,
+                 double* r_learned, int32_t* learned_used) {
+  if (!ctx || !o) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  if (!ctx->bcs_set) return fail(ctx, PFEM_ERR_STATE, "pfem_set_bcs must be called first");
+  cudaSetDevice(ctx->device);
+  StepTimes tm;
+  bool hf = false;
+  double r0 = 0;
+  int rc = step_begin(ctx, lambda, o, &tm, &hf, &r0);
+  if (rc) return rc;
+  const MlpState& ml = ctx->mlp;
+  if (r_extrap) *r_extrap = ml.last_r_ex;
+  if (r_learned) *r_learned = ml.last_r_ml;
+  if (learned_used) *learned_used = ml.last_used ? 1 : 0;
+  if (r_extrap && ml.last_r_ex < 0) {
+    rc = residual_system(ctx, o->precision, lambda, r_extrap, &tm.asm_ms);
+    if (rc) return rc;
+  }
+  if (U) CK(cudaMemcpy(U, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  return PFEM_OK;
 }
 
 int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res, int32_t* iters_per_step,

@@ -414,45 +414,74 @@ __global__ void nodal_alpha_kernel(long long ne, const int* __restrict__ elem, c
     atomicAdd(&an[n], s / (double)val[n]);
   }
 }
-__global__ void max_abs_diff_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b,
-                                    double* __restrict__ part) {
-  __shared__ double sh[32];
-  double m = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    m = fmax(m, fabs(a[i] - b[i]));
+constexpr int SCALE_BLOCKS = 1024;
+// per-block maxima of |dU_n| and |dU_n - rho dU_{n-1}| (dU_n = U0 - U1, dU_{n-1} = U1 - U2)
+__global__ void scales_kernel(long long n, const double* __restrict__ U0, const double* __restrict__ U1,
+                              const double* __restrict__ U2, double rho, double* __restrict__ part) {
+  __shared__ double sh[2][32];
+  double m1 = 0.0, m2 = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double d1 = U0[i] - U1[i];
+    m1 = fmax(m1, fabs(d1));
+    m2 = fmax(m2, fabs(d1 - rho * (U1[i] - U2[i])));
+  }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  for (int o = 16; o > 0; o >>= 1) {
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = m1;
+    sh[1][threadIdx.x >> 5] = m2;
+  }
   __syncthreads();
   if (threadIdx.x < 32) {
-    m = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    const bool in = threadIdx.x < (blockDim.x >> 5);
+    m1 = in ? sh[0][threadIdx.x] : 0.0;
+    m2 = in ? sh[1][threadIdx.x] : 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (threadIdx.x == 0) part[blockIdx.x] = m;
+    for (int o = 16; o > 0; o >>= 1) {
+      m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+      m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    if (threadIdx.x == 0) {
+      part[blockIdx.x] = m1;
+      part[SCALE_BLOCKS + blockIdx.x] = m2;
+    }
   }
 }
-__global__ void max_final_kernel(int np, const double* __restrict__ part, double* __restrict__ out) {
-  double m = 0.0;
-  for (int i = 0; i < np; ++i) m = fmax(m, part[i]);
-  *out = m > 1e-300 ? m : 1e-300;
+// scale[1] is floored at 1e-6 scale[0] so a purely linear response (zero
+// second difference) cannot blow the normalised features up.
+__global__ void scales_final_kernel(int np, const double* __restrict__ part, double* __restrict__ scale) {
+  double m1 = 0.0, m2 = 0.0;
+  for (int i = 0; i < np; ++i) {
+    m1 = fmax(m1, part[i]);
+    m2 = fmax(m2, part[SCALE_BLOCKS + i]);
+  }
+  m1 = fmax(m1, 1e-300);
+  scale[0] = m1;
+  scale[1] = fmax(m2, 1e-6 * m1);
 }
-// features of node n for the step to lam (dU_n = U0 - U1, dU_{n-1} = U1 - U2)
+// features of node n for the step to lam: position in the bounding box,
+// dU_n / scale[0], (dU_n - rho dU_{n-1}) / scale[1], nodal equivalent plastic
+// strain, load-step size, load factor
 __global__ void features_kernel(long long nn, const double* __restrict__ X, double lx, double ly, double lz,
                                 double ex, double ey, double ez, const double* __restrict__ U0,
                                 const double* __restrict__ U1, const double* __restrict__ U2,
-                                const double* __restrict__ an, double dlam, double lam,
+                                const double* __restrict__ an, double dlam, double lam, double rho,
                                 const double* __restrict__ scale, __nv_bfloat16* __restrict__ out) {
   const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= nn) return;
-  const double is = 1.0 / *scale;
+  const double is1 = 1.0 / scale[0], is2 = 1.0 / scale[1];
   float f[INP];
   f[0] = (float)((X[n * 3 + 0] - lx) / ex - 0.5);
   f[1] = (float)((X[n * 3 + 1] - ly) / ey - 0.5);
   f[2] = (float)((X[n * 3 + 2] - lz) / ez - 0.5);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    f[3 + d] = (float)((U0[n * 3 + d] - U1[n * 3 + d]) * is);
-    f[6 + d] = (float)((U1[n * 3 + d] - U2[n * 3 + d]) * is);
+    const double d1 = U0[n * 3 + d] - U1[n * 3 + d];
+    f[3 + d] = (float)(d1 * is1);
+    f[6 + d] = (float)((d1 - rho * (U1[n * 3 + d] - U2[n * 3 + d])) * is2);
   }
   f[9] = (float)(10.0 * an[n]);
   f[10] = (float)(10.0 * dlam);
@@ -467,13 +496,13 @@ __global__ void targets_kernel(long long nn, const double* __restrict__ Un, cons
                                float* __restrict__ out) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= nn * 3) return;
-  out[i] = (float)((Un[i] - U0[i] - r * (U0[i] - U1[i])) / *scale);
+  out[i] = (float)((Un[i] - U0[i] - r * (U0[i] - U1[i])) / scale[1]);
 }
 __global__ void apply_kernel(long long nn, const double* __restrict__ U0, const double* __restrict__ U1, double r,
                              const double* __restrict__ scale, const float* __restrict__ Y, double* __restrict__ U) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= nn * 3) return;
-  U[i] = U0[i] + r * (U0[i] - U1[i]) + *scale * (double)Y[i];
+  U[i] = U0[i] + r * (U0[i] - U1[i]) + scale[1] * (double)Y[i];
 }
 __global__ void random_rows_kernel(int n, long long nrows, unsigned long long seed, int* __restrict__ rows) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -492,19 +521,20 @@ void mlp_nodal_alpha(long long ne, long long nn, const int* elem, const double* 
   nodal_alpha_kernel<<<(int)((ne + 255) / 256), 256, 0, st>>>(ne, elem, alpha_gp, valence, anode);
 }
 void mlp_features(long long nn, const double* X, const double* lo, const double* ext, const double* U0,
-                  const double* U1, const double* U2, const double* anode, double dlam, double lam, double* scale,
-                  double* part, void* feat, cudaStream_t st) {
+                  const double* U1, const double* U2, const double* anode, double dlam, double lam, double rho,
+                  double* scale, double* part, void* feat, cudaStream_t st) {
   const long long n3 = nn * 3;
-  const int blocks = (int)std::min<long long>((n3 + 255) / 256, 1184);
+  const int blocks = (int)std::min<long long>((n3 + 255) / 256, SCALE_BLOCKS);
   count_launch();
-  max_abs_diff_kernel<<<blocks, 256, 0, st>>>(n3, U0, U1, part);
+  scales_kernel<<<blocks, 256, 0, st>>>(n3, U0, U1, U2, rho, part);
   count_launch();
-  max_final_kernel<<<1, 1, 0, st>>>(blocks, part, scale);
+  scales_final_kernel<<<1, 1, 0, st>>>(blocks, part, scale);
   count_launch();
   features_kernel<<<(int)((nn + 255) / 256), 256, 0, st>>>(nn, X, lo[0], lo[1], lo[2], ext[0], ext[1], ext[2], U0,
-                                                           U1, U2, anode, dlam, lam, scale,
+                                                           U1, U2, anode, dlam, lam, rho, scale,
                                                            static_cast<__nv_bfloat16*>(feat));
 }
+
 void mlp_targets(long long nn, const double* Unew, const double* U0, const double* U1, double r,
                  const double* scale, float* out, cudaStream_t st) {
   count_launch();

@@ -30,6 +30,9 @@ struct MlpState {
   bool recording = false;
   bool have_feat = false;    // features of the current step computed
   double r_ratio = 1.0;      // dlam_{n+1} / dlam_n of the current step
+  double last_r_ex = -1.0;   // FP64 residuals of the last prediction (-1: not evaluated)
+  double last_r_ml = -1.0;
+  bool last_used = false;    // the last prediction kept the learned guess
   int* rows = nullptr;       // batch row indices
   int rows_cap = 0;
 };
@@ -43,9 +46,11 @@ void mlp_pack_features(const float* f, long long n, void* out, cudaStream_t st);
 // solver-side helpers (mlp.cu)
 void mlp_nodal_alpha(long long ne, long long nn, const int* elem, const double* alpha_gp, const float* valence,
                      double* anode, cudaStream_t st);
+// scale[0] = max |dU_n|, scale[1] = max |dU_n - rho dU_{n-1}| (the second
+// difference); part needs 2048 doubles.
 void mlp_features(long long nn, const double* X, const double* lo, const double* ext, const double* U0,
-                  const double* U1, const double* U2, const double* anode, double dlam, double lam, double* scale,
-                  double* part, void* feat, cudaStream_t st);
+                  const double* U1, const double* U2, const double* anode, double dlam, double lam, double rho,
+                  double* scale, double* part, void* feat, cudaStream_t st);
 void mlp_targets(long long nn, const double* Unew, const double* U0, const double* U1, double r,
                  const double* scale, float* out, cudaStream_t st);
 void mlp_apply(long long nn, const double* U0, const double* U1, double r, const double* scale, const float* Y,

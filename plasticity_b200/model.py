@@ -249,7 +249,7 @@ class Model:
 
     def _opts(self, nsteps=10, tol=1e-8, maxiter=25, precision="fp64", linsolve="cg", lin_rtol=None,
               predictor="previous", amg_rebuild=False, cheb_degree=2, cg_itmax=200, eta_min=None,
-              line_search=False, verbose=False):
+              line_search=False, verbose=False, predictor_smooth=None):
         o = L.SolveOpts()
         L.lib().pfem_default_opts(C.byref(o))
         o.nsteps, o.maxiter, o.tol = nsteps, maxiter, tol
@@ -266,6 +266,8 @@ class Model:
         o.krylov_itmax = cg_itmax
         o.verbose = int(bool(verbose))
         o.line_search = int(bool(line_search))
+        if predictor_smooth is not None:
+            o.predictor_smooth = int(predictor_smooth)
         return o
 
     def solve(self, nsteps=10, tol=1e-8, maxiter=25, **kw) -> SolveResult:
@@ -297,6 +299,18 @@ class Model:
         rc = L.lib().pfem_newton(self._ctx, float(lam), C.byref(o), C.byref(it), ptr(hist), ptr(kh, L._i32))
         check(rc, self._ctx)
         return list(hist[:it.value]), list(kh[:max(it.value - 1, 0)])
+
+    def predict(self, lam, predictor="learned", **kw):
+        """Newton predictor for the load step to `lam` alone (no reference counterpart):
+        leaves the chosen guess as the current U and returns
+        (U, |R| extrapolated, |R| learned or None, learned guess kept)."""
+        self._push_bcs()
+        o = self._opts(predictor=predictor, **kw)
+        U = np.zeros(self.ndof)
+        rex, rml, used = C.c_double(), C.c_double(), C.c_int32()
+        check(L.lib().pfem_predict(self._ctx, float(lam), C.byref(o), ptr(U), C.byref(rex), C.byref(rml),
+                                   C.byref(used)), self._ctx)
+        return U, rex.value, (rml.value if rml.value >= 0 else None), bool(used.value)
 
     def residual(self, lam, precision="fp64"):
         """Assemble + impose at the current U (one newton! iteration's residual);

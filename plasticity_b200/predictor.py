@@ -47,28 +47,58 @@ def _path_model(n, device=0):
 
 
 def run_path(M, w, predictor, precision="mixed", tol=1e-8):
-    """Run one load path on an existing model with the path's BCs; returns stats."""
+    """Solve one load path on an existing model with the path's BCs; returns stats."""
+    w.apply(M)
+    t0 = time.perf_counter()
+    r = M.solve(nsteps=w.nsteps, tol=tol, maxiter=40, precision=precision, predictor=predictor,
+                line_search=True)
+    sec = time.perf_counter() - t0
+    return dict(converged=r.converged, newton=list(r.iters), krylov=[int(sum(k)) for k in r.cg_iters],
+                first_residual=[float(h[0]) for h in r.residuals], seconds=sec,
+                learned_used=int(r.stats["predictor_learned_used"]), stats=r.stats)
+
+
+def guess_errors(M, w, smooth=None, precision="mixed", tol=1e-10):
+    """Quality of the two guesses along one load path.  At every load step from
+    the third on (the learned guess needs two converged increments), both
+    guesses are formed, Newton converges from the one the FP64 residual picks,
+    and each guess's error is measured against the converged U as a fraction of
+    the step's increment.  Returns per-step rows."""
     w.apply(M)
     M.reset()
-    its, kry, res0 = [], [], []
-    t0 = time.perf_counter()
+    rows = []
+    U_prev = np.zeros(M.ndof)
+    kw = dict(precision=precision, line_search=True, tol=tol, maxiter=40)
+    sm = {} if smooth is None else dict(predictor_smooth=smooth)
     for s in range(1, w.nsteps + 1):
-        h, k = M.newton(s / w.nsteps, tol=tol, maxiter=40, precision=precision, predictor=predictor,
-                        line_search=True)
-        its.append(len(h)); kry.append(int(sum(k))); res0.append(float(h[0]))
-    return dict(newton=its, krylov=kry, first_residual=res0, seconds=time.perf_counter() - t0,
-                learned_used=None)
+        lam = s / w.nsteps
+        if s <= 2:
+            M.newton(lam, predictor="extrapolate", **kw)
+            U_prev = M.U
+            continue
+        U_ex, _, _, _ = M.predict(lam, "extrapolate", precision=precision)
+        U_ml, r_ex, r_ml, used = M.predict(lam, "learned", precision=precision, **sm)
+        h, k = M.newton(lam, predictor="previous", **kw)
+        U = M.U
+        inc = max(np.linalg.norm(U - U_prev), 1e-300)
+        rows.append(dict(step=s, r_extrap=r_ex, r_learned=r_ml, used=used, newton=len(h), krylov=int(sum(k)),
+                         err_extrap=float(np.linalg.norm(U_ex - U) / inc),
+                         err_chosen=float(np.linalg.norm(U_ml - U) / inc)))
+        U_prev = U
+    return rows
 
 
-def generate(M, n, paths, seed0=1000, nsteps=20):
-    """Record training pairs from `paths` solver-generated load paths."""
+def generate(M, n, paths, seed0=1000, nsteps=(20, 40)):
+    """Record training pairs from `paths` solver-generated load paths; path i
+    takes nsteps[i % len(nsteps)] increments, so the load-step-size input
+    varies across the set."""
     from . import workloads as W
-    cap = paths * (nsteps - 2) * M.nn
+    cap = sum(nsteps[i % len(nsteps)] - 2 for i in range(paths)) * M.nn
     M.mlp_init(0)
     M.mlp_record("start", cap)
     M.mlp_record("clear")
     for i in range(paths):
-        w = W.config4_path(n=n, nsteps=nsteps, seed=seed0 + i)
+        w = W.config4_path(n=n, nsteps=nsteps[i % len(nsteps)], seed=seed0 + i)
         run_path(M, w, "extrapolate")
     size = M.mlp_record("size")
     M.mlp_record("stop")
@@ -81,7 +111,8 @@ def train(M, steps, batch=65536, lr=1e-3, seed=0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train", "evaluate"])
+    ap.add_argument("cmd", choices=["train", "evaluate", "guess"])
+    ap.add_argument("--smooth", type=int, default=None)
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--paths", type=int, default=64)
     ap.add_argument("--steps", type=int, default=3000)
@@ -104,6 +135,19 @@ def main():
                     gen_seconds=t1 - t0, train_seconds=t2 - t1)
         np.savez(args.out, params=M.mlp_params(), meta=json.dumps(meta), losses=losses)
         print(json.dumps(meta))
+    elif args.cmd == "guess":
+        M = _path_model(args.n)
+        load_into(M, args.out)
+        allr = []
+        for i in range(args.paths):
+            allr += guess_errors(M, W.config4_path(n=args.n, seed=args.seed0 + i), args.smooth)
+        med = lambda k: float(np.median([r[k] for r in allr]))
+        print(json.dumps(dict(n=args.n, paths=args.paths, smooth=args.smooth, steps=len(allr),
+                              learned_kept=int(sum(r["used"] for r in allr)),
+                              median_err_extrap=med("err_extrap"), median_err_chosen=med("err_chosen"),
+                              median_r_extrap=med("r_extrap"), median_r_learned=med("r_learned"),
+                              newton=int(sum(r["newton"] for r in allr)),
+                              krylov=int(sum(r["krylov"] for r in allr)))))
     else:
         M = _path_model(args.n)
         have = weights_available(args.out)
@@ -111,16 +155,14 @@ def main():
         for pred in (["extrapolate", "learned"] if have else ["extrapolate"]):
             if pred == "learned":
                 load_into(M, args.out)
-            rows = []
-            for i in range(args.paths):
-                w = W.config4_path(n=args.n, seed=args.seed0 + i)
-                rows.append(run_path(M, w, pred))
-            out[pred] = dict(newton=int(sum(sum(r["newton"]) for r in rows)),
+            rows = [run_path(M, W.config4_path(n=args.n, seed=args.seed0 + i), pred) for i in range(args.paths)]
+            out[pred] = dict(converged=all(r["converged"] for r in rows),
+                             newton=int(sum(sum(r["newton"]) for r in rows)),
                              krylov=int(sum(sum(r["krylov"]) for r in rows)),
                              seconds=float(sum(r["seconds"] for r in rows)),
-                             mean_first_residual=float(np.mean([np.mean(r["first_residual"][2:]) for r in rows])))
+                             learned_used=int(sum(r["learned_used"] for r in rows)),
+                             steps=int(sum(len(r["newton"]) for r in rows)))
         print(json.dumps(out))
-
 
 if __name__ == "__main__":
     main()
