@@ -1124,7 +1124,7 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->cheb_degree = 2;
   o->verbose = 0;
   o->line_search = 0;
-  o->predictor_smooth = 4;
+  o->predictor_smooth = 16;
 }
 
 const char* pfem_last_error(const pfem_ctx* ctx) {

@@ -1,0 +1,67 @@
+"""Small, self-contained runs of the hot kernels, for profilers.
+
+Builds the jittered compression cube at n^3 (the 64^3 bench workload by
+default), sets a displacement that drives most Gauss points plastic (uniform
+1% compression plus seeded noise), then launches:
+
+  1. the mixed-precision assembly (element kernel per color, FP32 tangent) `reps` times,
+  2. the FP64 assembly `reps` times,
+  3. the level-0 FP32 block-CSR SpMV on that tangent `reps` times,
+  4. the predictor network's forward pass over one row per node `reps` times
+     (weights from plasticity_b200/weights when present, else random).
+
+Each family is timed with CUDA events on the library's stream and printed as one
+JSON line, so the same command serves a launch list, a single-kernel capture
+(`-k regex:element_color_kernel`, `bsr_spmv_kernel`, `mlp_tile_kernel`) and a
+quick timing.
+
+    python -m plasticity_b200.profile_case --n 64 --reps 3
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--strain", type=float, default=0.01)
+    args = ap.parse_args()
+
+    from . import model as P
+    from . import predictor as PR
+    from . import workloads as W
+
+    w = W.config2(n=args.n)
+    M = P.Model(w.mesh, P.J2Material(**w.material), sigy0_e=w.sigy0_e)
+    w.apply(M)
+    X = w.mesh.nodes
+    rng = np.random.default_rng(3)
+    U = np.stack([0.3 * args.strain * X[0], 0.3 * args.strain * X[1], -args.strain * X[2]]).T.reshape(-1)
+    U += 1e-2 * args.strain / args.n * rng.standard_normal(U.shape)
+    M.set_displacement(U)
+
+    out = {"n": args.n, "elements": w.mesh.nelem, "dofs": 3 * w.mesh.nnodes, "reps": args.reps}
+    out["assembly_mixed_ms"] = M.profile(1, reps=args.reps)
+    out["assembly_fp64_ms"] = M.profile(0, reps=args.reps)
+    out["spmv_fp32_ms"] = M.profile(2, reps=args.reps)
+    if PR.weights_available():
+        PR.load_into(M)
+    else:
+        M.mlp_init(0)
+    F = rng.standard_normal((M.nn, 12)).astype(np.float32)
+    M.mlp_forward(F)
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        M.mlp_forward(F)
+    out["mlp_forward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
