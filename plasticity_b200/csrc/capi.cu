@@ -38,6 +38,7 @@ struct KrylovWork {
   T* sc = nullptr;    // device scalars
   T* part = nullptr;  // reduction partials
   T* b = nullptr;
+  T *xa = nullptr, *b0 = nullptr;  // iterative refinement: accumulated solution, saved right-hand side
 };
 
 struct HostLevel {
@@ -570,6 +571,7 @@ int krylov_alloc(pfem_ctx* ctx) {
   CK(dalloc(ctx, &w.p, n)); CK(dalloc(ctx, &w.q, n)); CK(dalloc(ctx, &w.rh, n));
   CK(dalloc(ctx, &w.v, n)); CK(dalloc(ctx, &w.s, n)); CK(dalloc(ctx, &w.t, n));
   CK(dalloc(ctx, &w.ph, n)); CK(dalloc(ctx, &w.sh, n)); CK(dalloc(ctx, &w.b, n));
+  CK(dalloc(ctx, &w.xa, n)); CK(dalloc(ctx, &w.b0, n));
   CK(dalloc(ctx, &w.sc, 16)); CK(dalloc(ctx, &w.part, 2048));
   return PFEM_OK;
 }
@@ -729,7 +731,7 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
 // Preconditioned CG / BiCGStab on level-0 operator with the AMG V-cycle.
 // b and the result x live in kw.b / kw.x.  Returns iterations (>=0) or <0.
 template <typename T>
-int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* conv) {
+int krylov_inner(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* conv) {
   Amg<T>& A = amg_of<T>(ctx);
   KrylovWork<T>& w = kw_of<T>(ctx);
   const BsrMat<T>& K = A.lv[0].A;
@@ -783,15 +785,72 @@ int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* 
       dot<T>(n, w.t, w.t, w.sc + 6, w.part, st, false);
       bicg_xr<T>(n, w.sc, w.ph, w.sh, w.s, w.t, w.x, w.r, st);
       pfem::count_launch(); bicg_finish_kernel<T><<<1, 1, 0, st>>>(w.sc);
-      dot<T>(n, w.r, w.r, w.sc + 3, w.part, st, true);
+      // |r| goes to slot 7: slot 3 holds omega for the next iteration's beta
+      dot<T>(n, w.r, w.r, w.sc + 7, w.part, st, true);
       T rn = 0;
-      CK(cudaMemcpyAsync(&rn, w.sc + 3, sizeof(T), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(&rn, w.sc + 7, sizeof(T), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       *iters = it;
       if ((double)rn <= thr) { *conv = true; break; }
       if (!std::isfinite((double)rn)) break;
     }
   }
+  CKL();
+  return PFEM_OK;
+}
+
+// Solve K x = b (kw.b -> kw.x) to relative tolerance rtol.  Below the level a
+// recursively updated Krylov residual reliably reaches in precision T (1e-8 in
+// FP64, 1e-5 in FP32 -- the F-bar tangent is nonsymmetric, so CG and
+// BiCGStab drift from the true residual there), the inner method runs inside
+// an iterative-refinement loop: x += inner solve of K d = b - K x, with the
+// residual recomputed from K each pass.
+template <typename T>
+int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* conv) {
+  const double floor_rtol = std::is_same<T, double>::value ? 1e-8 : 1e-5;
+  if (rtol >= floor_rtol) return krylov_inner<T>(ctx, method, rtol, itmax, iters, conv);
+  Amg<T>& A = amg_of<T>(ctx);
+  KrylovWork<T>& w = kw_of<T>(ctx);
+  const BsrMat<T>& K = A.lv[0].A;
+  const long long n = ctx->ndof;
+  cudaStream_t st = ctx->st;
+  CK(cudaMemcpyAsync(w.b0, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  fill<T>(n, w.xa, T(0), st);
+  dot<T>(n, w.b0, w.b0, w.sc + 12, w.part, st, true);
+  T bn = 0;
+  CK(cudaMemcpyAsync(&bn, w.sc + 12, sizeof(T), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *iters = 0;
+  *conv = false;
+  if (!(bn > 0)) {
+    fill<T>(n, w.x, T(0), st);
+    *conv = true;
+    return PFEM_OK;
+  }
+  const double target = rtol * (double)bn;
+  double rn = (double)bn;
+  for (int pass = 0; pass < 8 && *iters < itmax; ++pass) {
+    int it = 0;
+    bool c = false;
+    const double rel = std::max(floor_rtol, target / rn);
+    int rc = krylov_inner<T>(ctx, method, rel, itmax - *iters, &it, &c);
+    if (rc) return rc;
+    *iters += it;
+    axpby<T>(n, T(1), w.x, T(1), w.xa, st);
+    bsr_residual<T>(K, w.xa, w.b0, w.b, st);  // next right-hand side: the true residual
+    dot<T>(n, w.b, w.b, w.sc + 12, w.part, st, true);
+    T r = 0;
+    CK(cudaMemcpyAsync(&r, w.sc + 12, sizeof(T), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    rn = (double)r;
+    if (!std::isfinite(rn)) break;
+    if (rn <= target) {
+      *conv = true;
+      break;
+    }
+  }
+  CK(cudaMemcpyAsync(w.x, w.xa, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(w.b, w.b0, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
   CKL();
   return PFEM_OK;
 }

@@ -4,15 +4,19 @@
 // Gauss point g of element `slot`: geometry, F / F-bar, trial b^e and its
 // eigenbasis, the J2 radial return in principal stresses, P = tau F^-T and the
 // two-point tangent A = dP/dFbar built column by column in the eigenbasis of
-// b^e.  It leaves (w s A, w s/3 A vec(F), F^-1, dN/dX) in shared memory and
-// writes the Kirchhoff stress, the elastic/plastic flag and -- on the commit
-// pass -- the exponential-map plastic update.  Phase B: lanes 0..23 each own
-// one column (b,k) of Ke and sum the eight Gauss-point contributions
+// b^e.  The internal force is summed over the element's eight Gauss-point
+// lanes node by node with warp shuffles (FP64) and added into R; the tangent
+// records (dN/dX, w s A, w s/3 A vec(F), F^-1) go to shared memory in the
+// tangent's type TT (FP32 on the mixed-precision path, where only the tangent
+// is FP32).  The Kirchhoff stress and the elastic/plastic flag are written,
+// and on the commit pass the exponential-map plastic update.  Phase B: the
+// 4 x 24 columns (b,k) of the warp's four element tangents are spread over the
+// 32 lanes; each sums the eight Gauss-point contributions
 //   Ke[:,(b,k)] = sum_g G_g^T (w s A G_g + (w s/3) A vec(F) (g0 - gJ)^T)[:,(b,k)]
-// (lagrangian/src/Elements.jl:470-478 with _fbar_Geff :524-531), then add them
-// into the 3x3-block CSR tangent in place; lanes 24..31 add Fe into R.  Elements
-// of one color share no node, so the adds need no atomics
-// (lagrangian/src/Assembly.jl:167-188, :370-385).
+// (lagrangian/src/Elements.jl:470-478 with _fbar_Geff :524-531) and adds them
+// into the 3x3-block CSR tangent in place.  Elements of one color share no
+// node, so the adds need no atomics (lagrangian/src/Assembly.jl:167-188,
+// :370-385).
 //
 // Arithmetic follows the reference kernel element_force_tangent_finite!
 // (Elements.jl:405-494), finite_kinematics (FiniteStrain.jl:148-170),
@@ -27,11 +31,18 @@
 
 namespace pfem {
 
-constexpr int EPW = 4;           // elements per warp
-constexpr int GPREC = 24 + 81 + 9 + 9;   // dNdX, w s A, w s/3 A vec(F), F^-1
-constexpr int SLOT = 48 + 24 + 8 * GPREC;  // Xe, ue, g0, GP records
-constexpr int WARP_SMEM = EPW * SLOT;      // doubles per warp
-constexpr int WPB = 1;           // warps per block
+constexpr int EPW = 4;                     // elements per warp
+constexpr int GPREC = 24 + 81 + 9 + 9;     // dNdX, w s A, w s/3 A vec(F), F^-1 (TT each)
+constexpr int SLOT_TT = 24 + 8 * GPREC;    // g0, then the 8 Gauss-point records
+constexpr int WPB = 1;                     // warps per block
+// Shared memory per warp (bytes).  The element's nodal coordinates and
+// displacements (48 doubles) live at the start of the record area until the
+// geometry is formed, then the records overwrite them.
+template <typename TT>
+constexpr int warp_smem_bytes(bool commit) {
+  return commit ? EPW * 48 * 8 : EPW * SLOT_TT * (int)sizeof(TT);
+}
+static_assert(8 * GPREC * 4 >= 48 * 8, "coordinate scratch must fit in the record area");
 
 __device__ __forceinline__ double nsgn_x(int a) { return (((a + 1) >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double nsgn_y(int a) { return ((a >> 1) & 1) ? 1.0 : -1.0; }
@@ -48,9 +59,9 @@ __device__ __forceinline__ void dshape_a(int a, double x, double y, double z, do
 template <typename KT, bool COMMIT, bool FBAR>
 __global__ void __launch_bounds__(32 * WPB)
 element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
-  extern __shared__ double smem[];
+  using TT = KT;  // type of the tangent records and of the phase-B arithmetic
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* ws = smem + warp * WARP_SMEM;
   const int slot = lane >> 3, g = lane & 7;
   const long long li = ((long long)blockIdx.x * WPB + warp) * EPW + slot;
   const bool valid = li < nlist;
@@ -58,15 +69,14 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   // first element (so every lane takes part in the warp shuffles) and write
   // nothing to global memory.
   const int e = elist[valid ? li : 0];
-  double* S = ws + slot * SLOT;
-  double* Xe = S;           // [a*3+d]
-  double* ue = S + 24;      // [a*3+d]
-  double* g0s = S + 48;     // [a*3+k]
-  double* R = S + 72 + g * GPREC;
-  double* dNdX = R;         // [a*3+j]
-  double* As = R + 24;      // [(j*3+i)*9 + (q*3+p)]
-  double* uv = R + 105;     // [j*3+i]
-  double* Fiu = R + 114;    // F^-1 of the standard F, row-major
+  TT* const wbase = reinterpret_cast<TT*>(smem_raw) + warp * EPW * SLOT_TT;
+  TT* const S = wbase + slot * SLOT_TT;
+  TT* const g0s = S;                      // [a*3+k]
+  TT* const Rg = S + 24 + g * GPREC;      // this lane's Gauss-point record
+  double* const XU = COMMIT ? reinterpret_cast<double*>(smem_raw) + (warp * EPW + slot) * 48
+                            : reinterpret_cast<double*>(S + 24);
+  double* const Xe = XU;                  // [a*3+d]
+  double* const ue = XU + 24;             // [a*3+d]
 
   __shared__ int nodes_s[WPB][EPW][8];
   {
@@ -82,38 +92,40 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
 
   const MatParams m = p.mat;
   const long long gp = (long long)e * 8 + g;
-  double scale = 1.0, w = 0.0;
-  {
-    // ---- F-bar centroid quantities (Elements.jl:418-424) ----
-    double J0 = 1.0;
-    double H0[9];  // J0mat^-1 F0^-1  (g0_(a,k) = sum_m DNC[a][m] H0[m][k])
-    if (FBAR) {
-      double J0m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, UC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double gc = 0.57735026918962576451;  // 1/sqrt(3)
+  const double xg = nsgn_x(g) * gc, yg = nsgn_y(g) * gc, zg = nsgn_z(g) * gc;
+  // ---- F-bar centroid quantities (Elements.jl:418-424) ----
+  double J0 = 1.0;
+  if (FBAR) {
+    double J0m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, UC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        double dc[3];
-        dshape_a(a, 0.0, 0.0, 0.0, dc);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            J0m[3 * i + j] += Xe[a * 3 + i] * dc[j];
-            UC[3 * i + j] += ue[a * 3 + i] * dc[j];
-          }
-      }
-      double J0i[9], F0[9], F0i[9];
-      inv3(J0m, J0i);
+    for (int a = 0; a < 8; ++a) {
+      double dc[3];
+      dshape_a(a, 0.0, 0.0, 0.0, dc);
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-          double s = (i == j) ? 1.0 : 0.0;
-#pragma unroll
-          for (int q = 0; q < 3; ++q) s += UC[3 * i + q] * J0i[3 * q + j];
-          F0[3 * i + j] = s;
+          J0m[3 * i + j] += Xe[a * 3 + i] * dc[j];
+          UC[3 * i + j] += ue[a * 3 + i] * dc[j];
         }
-      J0 = det3(F0);
+    }
+    double J0i[9], F0[9], F0i[9];
+    inv3(J0m, J0i);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double s = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s += UC[3 * i + q] * J0i[3 * q + j];
+        F0[3 * i + j] = s;
+      }
+    J0 = det3(F0);
+    if (!COMMIT && g == 0) {
+      // g0_(a,k) = sum_m dN_a/dxi_m(0) H0[m][k], H0 = J0mat^-1 F0^-1
       inv3(F0, F0i);
+      double H0[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -123,340 +135,336 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
           for (int q = 0; q < 3; ++q) s += J0i[3 * i + q] * F0i[3 * q + j];
           H0[3 * i + j] = s;
         }
-      if (g == 0) {
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          double dc[3];
-          dshape_a(a, 0.0, 0.0, 0.0, dc);
-#pragma unroll
-          for (int k = 0; k < 3; ++k)
-            g0s[a * 3 + k] = dc[0] * H0[k] + dc[1] * H0[3 + k] + dc[2] * H0[6 + k];
-        }
-      }
-    }
-    // ---- Gauss-point geometry: J = Xe' dN, dN/dX = dN J^-1 (Elements.jl:89,155-161) ----
-    const double gc = 0.57735026918962576451;  // 1/sqrt(3)
-    const double xg = nsgn_x(g) * gc, yg = nsgn_y(g) * gc, zg = nsgn_z(g) * gc;
-    double Jm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Ug[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      double d[3];
-      dshape_a(a, xg, yg, zg, d);
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          Jm[3 * i + j] += Xe[a * 3 + i] * d[j];
-          Ug[3 * i + j] += ue[a * 3 + i] * d[j];
-        }
-    }
-    w = det3(Jm);  // detJ * weight (weights are 1, Elements.jl:43)
-    double Ji[9];
-    inv3(Jm, Ji);
-    if (!COMMIT) {
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
-        double d[3];
-        dshape_a(a, xg, yg, zg, d);
+        double dc[3];
+        dshape_a(a, 0.0, 0.0, 0.0, dc);
 #pragma unroll
-        for (int j = 0; j < 3; ++j) dNdX[a * 3 + j] = d[0] * Ji[j] + d[1] * Ji[3 + j] + d[2] * Ji[6 + j];
+        for (int k = 0; k < 3; ++k) g0s[a * 3 + k] = (TT)(dc[0] * H0[k] + dc[1] * H0[3 + k] + dc[2] * H0[6 + k]);
       }
     }
-    // F = I + sum_a u_a (x) dN_a/dX  (FiniteStrain.jl:107-119)
-    double F[9];
+  }
+  // ---- Gauss-point geometry: J = Xe' dN (Elements.jl:89,155-161) ----
+  double Jm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Ug[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double d[3];
+    dshape_a(a, xg, yg, zg, d);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        double s = (i == j) ? 1.0 : 0.0;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) s += Ug[3 * i + q] * Ji[3 * q + j];
-        F[3 * i + j] = s;
+        Jm[3 * i + j] += Xe[a * 3 + i] * d[j];
+        Ug[3 * i + j] += ue[a * 3 + i] * d[j];
       }
-    const double Jg = det3(F);
-    scale = FBAR ? cbrt(J0 / Jg) : 1.0;  // Elements.jl:437
-    double Fb[9];
+  }
+  // The nodal coordinates are dead from here on; the records may overwrite them.
+  __syncwarp();
+  const double w = det3(Jm);  // detJ * weight (weights are 1, Elements.jl:43)
+  double Ji[9];
+  inv3(Jm, Ji);
+  // F = I + sum_a u_a (x) dN_a/dX  (FiniteStrain.jl:107-119)
+  double F[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Fb[i] = scale * F[i];
-    // ---- finite_kinematics (FiniteStrain.jl:148-170) ----
-    const double Jb = det3(Fb);
-    double c6[6];
+  for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int c = 0; c < 6; ++c) c6[c] = p.cpi[(long long)c * p.ngp + gp];
-    const double Cp[9] = {c6[0], c6[3], c6[5], c6[3], c6[1], c6[4], c6[5], c6[4], c6[2]};
-    double M[9];  // Cp Fb^T
+    for (int j = 0; j < 3; ++j) {
+      double s = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) s += Ug[3 * i + q] * Ji[3 * q + j];
+      F[3 * i + j] = s;
+    }
+  const double Jg = det3(F);
+  const double scale = FBAR ? cbrt(J0 / Jg) : 1.0;  // Elements.jl:437
+  double Fb[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Fb[i] = scale * F[i];
+  // ---- finite_kinematics (FiniteStrain.jl:148-170) ----
+  const double Jb = det3(Fb);
+  double c6[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) c6[c] = p.cpi[(long long)c * p.ngp + gp];
+  const double Cp[9] = {c6[0], c6[3], c6[5], c6[3], c6[1], c6[4], c6[5], c6[4], c6[2]};
+  double M[9];  // Cp Fb^T
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) M[3 * i + j] = Cp[3 * i] * Fb[3 * j] + Cp[3 * i + 1] * Fb[3 * j + 1] + Cp[3 * i + 2] * Fb[3 * j + 2];
+  double be[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) be[3 * i + j] = Fb[3 * i] * M[j] + Fb[3 * i + 1] * M[3 + j] + Fb[3 * i + 2] * M[6 + j];
+  be[1] = be[3] = 0.5 * (be[1] + be[3]);
+  be[2] = be[6] = 0.5 * (be[2] + be[6]);
+  be[5] = be[7] = 0.5 * (be[5] + be[7]);
+  double bv[3], Q[9];
+  const bool ok = Jb > 0.0;
+  if (!ok) {
+    if (valid && atomicCAS(&p.status->code, 0, 1) == 0) {
+      p.status->e = (long long)e + 1;
+      p.status->g = g + 1;
+      p.status->J = Jb;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Q[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    bv[0] = bv[1] = bv[2] = 1.0;
+  } else {
+    eig3_jacobi(be, bv, Q);
+  }
+  // ---- return_map on principal values (Materials.jl:159-250) ----
+  const double G = m.G, lam = m.lam, H = m.Hiso;
+  const double sy0 = p.sigy0_e ? p.sigy0_e[e] : m.sigy0;
+  const double an = p.alpha[gp];
+  const double e0 = 0.5 * log(bv[0]), e1 = 0.5 * log(bv[1]), e2 = 0.5 * log(bv[2]);
+  const double tre = e0 + e1 + e2;
+  const double t0 = lam * tre + 2.0 * G * e0, t1 = lam * tre + 2.0 * G * e1, t2 = lam * tre + 2.0 * G * e2;
+  const double pm = (t0 + t1 + t2) / 3.0;
+  const double s0 = t0 - pm, s1 = t1 - pm, s2 = t2 - pm;
+  const double nrm = sqrt(s0 * s0 + s1 * s1 + s2 * s2);
+  const double s32 = 1.22474487139158904910;  // sqrt(1.5)
+  const double qtr = s32 * nrm;
+  const double ftr = qtr - (sy0 + H * an);
+  const bool plastic = ftr > 0.0;
+  double n0 = 0.0, n1 = 0.0, n2 = 0.0, dg = 0.0, b0 = 0.0, g0c = 0.0;
+  double ta0 = t0, ta1 = t1, ta2 = t2;
+  if (plastic) {
+    n0 = s0 / nrm; n1 = s1 / nrm; n2 = s2 / nrm;
+    dg = ftr / (3.0 * G + H);
+    const double c = 2.0 * G * dg * s32;
+    ta0 = t0 - c * n0; ta1 = t1 - c * n1; ta2 = t2 - c * n2;
+    b0 = 2.0 * G * dg / qtr;
+    g0c = 2.0 * G / (3.0 * G + H);
+  }
+  // tau = Q diag(tau_A) Q^T  (Kirchhoff, physical-shear Voigt)
+  double tau[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) {
+      const double v = Q[3 * i] * ta0 * Q[3 * j] + Q[3 * i + 1] * ta1 * Q[3 * j + 1] + Q[3 * i + 2] * ta2 * Q[3 * j + 2];
+      tau[3 * i + j] = v;
+      tau[3 * j + i] = v;
+    }
+  if (valid) {
+    p.tau[0 * p.ngp + gp] = tau[0];
+    p.tau[1 * p.ngp + gp] = tau[4];
+    p.tau[2 * p.ngp + gp] = tau[8];
+    p.tau[3 * p.ngp + gp] = tau[1];
+    p.tau[4 * p.ngp + gp] = tau[5];
+    p.tau[5 * p.ngp + gp] = tau[2];
+    p.flags[gp] = plastic ? 1 : 0;
+  }
+  double Fbi[9];
+  inv3(Fb, Fbi);
+  if constexpr (COMMIT) {
+    if (!valid) return;
+    // exponential-map update b^e_{n+1} = exp(2 eps^e), Cp^-1 = F^-1 b^e F^-T
+    // (FiniteStrain.jl:331-343); eps^e shares the trial eigenbasis.
+    const double c = dg * s32;
+    const double l0 = exp(2.0 * (e0 - c * n0)), l1 = exp(2.0 * (e1 - c * n1)), l2 = exp(2.0 * (e2 - c * n2));
+    double T[9];  // Fbi Q
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) M[3 * i + j] = Cp[3 * i] * Fb[3 * j] + Cp[3 * i + 1] * Fb[3 * j + 1] + Cp[3 * i + 2] * Fb[3 * j + 2];
-    double be[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) be[3 * i + j] = Fb[3 * i] * M[j] + Fb[3 * i + 1] * M[3 + j] + Fb[3 * i + 2] * M[6 + j];
-    be[1] = be[3] = 0.5 * (be[1] + be[3]);
-    be[2] = be[6] = 0.5 * (be[2] + be[6]);
-    be[5] = be[7] = 0.5 * (be[5] + be[7]);
-    double bv[3], Q[9];
-    const bool ok = Jb > 0.0;
-    if (!ok) {
-      if (valid && atomicCAS(&p.status->code, 0, 1) == 0) {
-        p.status->e = (long long)e + 1;
-        p.status->g = g + 1;
-        p.status->J = Jb;
-      }
-#pragma unroll
-      for (int i = 0; i < 9; ++i) Q[i] = (i % 4 == 0) ? 1.0 : 0.0;
-      bv[0] = bv[1] = bv[2] = 1.0;
-    } else {
-      eig3_jacobi(be, bv, Q);
-    }
-    // ---- return_map on principal values (Materials.jl:159-250) ----
-    const double G = m.G, lam = m.lam, H = m.Hiso;
-    const double sy0 = p.sigy0_e ? p.sigy0_e[e] : m.sigy0;
-    const double an = p.alpha[gp];
-    const double e0 = 0.5 * log(bv[0]), e1 = 0.5 * log(bv[1]), e2 = 0.5 * log(bv[2]);
-    const double tre = e0 + e1 + e2;
-    const double t0 = lam * tre + 2.0 * G * e0, t1 = lam * tre + 2.0 * G * e1, t2 = lam * tre + 2.0 * G * e2;
-    const double pm = (t0 + t1 + t2) / 3.0;
-    const double s0 = t0 - pm, s1 = t1 - pm, s2 = t2 - pm;
-    const double nrm = sqrt(s0 * s0 + s1 * s1 + s2 * s2);
-    const double s32 = 1.22474487139158904910;  // sqrt(1.5)
-    const double qtr = s32 * nrm;
-    const double ftr = qtr - (sy0 + H * an);
-    const bool plastic = ftr > 0.0;
-    double n0 = 0.0, n1 = 0.0, n2 = 0.0, dg = 0.0, b0 = 0.0, g0c = 0.0;
-    double ta0 = t0, ta1 = t1, ta2 = t2;
-    if (plastic) {
-      n0 = s0 / nrm; n1 = s1 / nrm; n2 = s2 / nrm;
-      dg = ftr / (3.0 * G + H);
-      const double c = 2.0 * G * dg * s32;
-      ta0 = t0 - c * n0; ta1 = t1 - c * n1; ta2 = t2 - c * n2;
-      b0 = 2.0 * G * dg / qtr;
-      g0c = 2.0 * G / (3.0 * G + H);
-    }
-    // tau = Q diag(tau_A) Q^T  (Kirchhoff, physical-shear Voigt)
-    double tau[9];
+      for (int A = 0; A < 3; ++A) T[3 * i + A] = Fbi[3 * i] * Q[A] + Fbi[3 * i + 1] * Q[3 + A] + Fbi[3 * i + 2] * Q[6 + A];
+    double cn[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = i; j < 3; ++j) {
-        const double v = Q[3 * i] * ta0 * Q[3 * j] + Q[3 * i + 1] * ta1 * Q[3 * j + 1] + Q[3 * i + 2] * ta2 * Q[3 * j + 2];
-        tau[3 * i + j] = v;
-        tau[3 * j + i] = v;
+        const double v = T[3 * i] * l0 * T[3 * j] + T[3 * i + 1] * l1 * T[3 * j + 1] + T[3 * i + 2] * l2 * T[3 * j + 2];
+        cn[3 * i + j] = v;
+        cn[3 * j + i] = v;
       }
-    if (valid) {
-      p.tau[0 * p.ngp + gp] = tau[0];
-      p.tau[1 * p.ngp + gp] = tau[4];
-      p.tau[2 * p.ngp + gp] = tau[8];
-      p.tau[3 * p.ngp + gp] = tau[1];
-      p.tau[4 * p.ngp + gp] = tau[5];
-      p.tau[5 * p.ngp + gp] = tau[2];
-      p.flags[gp] = plastic ? 1 : 0;
+    p.cpi[0 * p.ngp + gp] = cn[0];
+    p.cpi[1 * p.ngp + gp] = cn[4];
+    p.cpi[2 * p.ngp + gp] = cn[8];
+    p.cpi[3 * p.ngp + gp] = cn[1];
+    p.cpi[4 * p.ngp + gp] = cn[5];
+    p.cpi[5 * p.ngp + gp] = cn[2];
+    p.alpha[gp] = an + dg;
+    // accumulated plastic strain (diagnostic; engineering-shear Voigt)
+    double nn_[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        nn_[3 * i + j] = c * (Q[3 * i] * n0 * Q[3 * j] + Q[3 * i + 1] * n1 * Q[3 * j + 1] + Q[3 * i + 2] * n2 * Q[3 * j + 2]);
+    p.epsp[0 * p.ngp + gp] += nn_[0];
+    p.epsp[1 * p.ngp + gp] += nn_[4];
+    p.epsp[2 * p.ngp + gp] += nn_[8];
+    p.epsp[3 * p.ngp + gp] += 2.0 * nn_[1];
+    p.epsp[4 * p.ngp + gp] += 2.0 * nn_[5];
+    p.epsp[5 * p.ngp + gp] += 2.0 * nn_[2];
+  } else {
+    // ---- P = tau Fb^-T (FiniteStrain.jl:560-561) ----
+    double P[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P[3 * i + j] = tau[3 * i] * Fbi[3 * j] + tau[3 * i + 1] * Fbi[3 * j + 1] + tau[3 * i + 2] * Fbi[3 * j + 2];
+    // ---- internal force, node by node: dN_a/dX = dN_a/dxi J^-1, then
+    // Fe_a = sum over the element's 8 Gauss-point lanes of w P dN_a/dX (FP64);
+    // lane g keeps node a = g and adds it into R (colored: no atomics).
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      double d[3];
+      dshape_a(a, xg, yg, zg, d);
+      const double x0 = d[0] * Ji[0] + d[1] * Ji[3] + d[2] * Ji[6];
+      const double x1 = d[0] * Ji[1] + d[1] * Ji[4] + d[2] * Ji[7];
+      const double x2 = d[0] * Ji[2] + d[1] * Ji[5] + d[2] * Ji[8];
+      Rg[a * 3 + 0] = (TT)x0;
+      Rg[a * 3 + 1] = (TT)x1;
+      Rg[a * 3 + 2] = (TT)x2;
+      double v0 = w * (P[0] * x0 + P[1] * x1 + P[2] * x2);
+      double v1 = w * (P[3] * x0 + P[4] * x1 + P[5] * x2);
+      double v2 = w * (P[6] * x0 + P[7] * x1 + P[8] * x2);
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+        v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+      }
+      if (a == g) { f0 = v0; f1 = v1; f2 = v2; }
     }
-    double Fbi[9];
-    inv3(Fb, Fbi);
-    if (COMMIT && valid) {
-      // exponential-map update b^e_{n+1} = exp(2 eps^e), Cp^-1 = F^-1 b^e F^-T
-      // (FiniteStrain.jl:331-343); eps^e shares the trial eigenbasis.
-      const double c = dg * s32;
-      const double l0 = exp(2.0 * (e0 - c * n0)), l1 = exp(2.0 * (e1 - c * n1)), l2 = exp(2.0 * (e2 - c * n2));
-      double T[9];  // Fbi Q
+    if (valid) {
+      const int nd = nodes_s[warp][slot][g];
+      p.R[(long long)nd * 3 + 0] += f0;
+      p.R[(long long)nd * 3 + 1] += f1;
+      p.R[(long long)nd * 3 + 2] += f2;
+    }
+    // ---- A = dP/dFbar in the eigenbasis of b^e (dPdF, FiniteStrain.jl:503-547) ----
+    // gamma_AB of _dhalflog_contract (FiniteStrain.jl:463-482)
+    const double lyv[3] = {e0, e1, e2};
+    TT gam[9];
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
+    for (int A = 0; A < 3; ++A)
 #pragma unroll
-        for (int A = 0; A < 3; ++A) T[3 * i + A] = Fbi[3 * i] * Q[A] + Fbi[3 * i + 1] * Q[3 + A] + Fbi[3 * i + 2] * Q[6 + A];
-      double cn[9];
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = i; j < 3; ++j) {
-          const double v = T[3 * i] * l0 * T[3 * j] + T[3 * i + 1] * l1 * T[3 * j + 1] + T[3 * i + 2] * l2 * T[3 * j + 2];
-          cn[3 * i + j] = v;
-          cn[3 * j + i] = v;
-        }
-      p.cpi[0 * p.ngp + gp] = cn[0];
-      p.cpi[1 * p.ngp + gp] = cn[4];
-      p.cpi[2 * p.ngp + gp] = cn[8];
-      p.cpi[3 * p.ngp + gp] = cn[1];
-      p.cpi[4 * p.ngp + gp] = cn[5];
-      p.cpi[5 * p.ngp + gp] = cn[2];
-      p.alpha[gp] = an + dg;
-      // accumulated plastic strain (diagnostic; engineering-shear Voigt)
-      double nn_[9];
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-          nn_[3 * i + j] = c * (Q[3 * i] * n0 * Q[3 * j] + Q[3 * i + 1] * n1 * Q[3 * j + 1] + Q[3 * i + 2] * n2 * Q[3 * j + 2]);
-      p.epsp[0 * p.ngp + gp] += nn_[0];
-      p.epsp[1 * p.ngp + gp] += nn_[4];
-      p.epsp[2 * p.ngp + gp] += nn_[8];
-      p.epsp[3 * p.ngp + gp] += 2.0 * nn_[1];
-      p.epsp[4 * p.ngp + gp] += 2.0 * nn_[5];
-      p.epsp[5 * p.ngp + gp] += 2.0 * nn_[2];
-    } else if (!COMMIT) {
-      // ---- P = tau Fb^-T (FiniteStrain.jl:560-561) and Fe_g ----
-      double P[9];
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) P[3 * i + j] = tau[3 * i] * Fbi[3 * j] + tau[3 * i + 1] * Fbi[3 * j + 1] + tau[3 * i + 2] * Fbi[3 * j + 2];
-      double fe[24];
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-          fe[a * 3 + i] = w * (P[3 * i] * dNdX[a * 3] + P[3 * i + 1] * dNdX[a * 3 + 1] + P[3 * i + 2] * dNdX[a * 3 + 2]);
-      // sum over the 8 Gauss-point lanes of this element
-#pragma unroll
-      for (int k = 0; k < 24; ++k) {
-        double v = fe[k];
-        v += __shfl_xor_sync(0xffffffffu, v, 1);
-        v += __shfl_xor_sync(0xffffffffu, v, 2);
-        v += __shfl_xor_sync(0xffffffffu, v, 4);
-        fe[k] = v;
+      for (int B = 0; B < 3; ++B) {
+        double v;
+        if (A == B) v = 1.0 / (2.0 * bv[A]);
+        else if (fabs(bv[A] - bv[B]) < 1e-9 * (fabs(bv[A]) + fabs(bv[B]) + 1.0)) v = 1.0 / (bv[A] + bv[B]);
+        else v = (lyv[A] - lyv[B]) / (bv[A] - bv[B]);
+        gam[3 * A + B] = (TT)v;
       }
-      // lane g adds the forces of node a = g (colored: no atomics)
-      {
-        const int nd = nodes_s[warp][slot][g];
-        double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    TT Qt[9], MQ[9], NN[9], FbiT[9], Pt[9], Ft[9];  // MQ = (Cp Fb^T) Q, NN = Q^T Fb^-T
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
-          if (a == g) { f0 = fe[a * 3]; f1 = fe[a * 3 + 1]; f2 = fe[a * 3 + 2]; }
-        if (valid) {
-          p.R[(long long)nd * 3 + 0] += f0;
-          p.R[(long long)nd * 3 + 1] += f1;
-          p.R[(long long)nd * 3 + 2] += f2;
-        }
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        FbiT[3 * i + j] = (TT)Fbi[3 * j + i];
+        Qt[3 * i + j] = (TT)Q[3 * i + j];
+        Pt[3 * i + j] = (TT)P[3 * i + j];
+        Ft[3 * i + j] = (TT)F[3 * i + j];
       }
-      // ---- A = dP/dFbar in the eigenbasis of b^e (dPdF, FiniteStrain.jl:503-547) ----
-      // gamma_AB of _dhalflog_contract (FiniteStrain.jl:463-482)
-      const double lyv[3] = {e0, e1, e2};
-      double gam[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int B = 0; B < 3; ++B) {
+        MQ[3 * i + B] = (TT)(M[3 * i] * Q[B] + M[3 * i + 1] * Q[3 + B] + M[3 * i + 2] * Q[6 + B]);
+        NN[3 * i + B] = (TT)(Q[i] * Fbi[3 * B] + Q[3 + i] * Fbi[3 * B + 1] + Q[6 + i] * Fbi[3 * B + 2]);
+      }
+    // tangent modulus D in principal form:
+    //   dtau' = c2 Y + c1 tr(Y) I + c3 (n . diag Y) diag(n)
+    const TT c2 = (TT)(2.0 * G - 3.0 * G * b0);
+    const TT c1 = (TT)(lam + G * b0);
+    const TT c3 = (TT)(3.0 * G * (b0 - g0c));
+    const TT nv[3] = {(TT)n0, (TT)n1, (TT)n2};
+    const TT ws_ = (TT)(w * scale);
+    TT* const As = Rg + 24;  // [(j*3+i)*9 + (q*3+p)]
+    TT uacc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int col = 0; col < 9; ++col) {
+      const int pp = col % 3, qq = col / 3;
+      TT Y[9];
 #pragma unroll
       for (int A = 0; A < 3; ++A)
 #pragma unroll
-        for (int B = 0; B < 3; ++B) {
-          double v;
-          if (A == B) v = 1.0 / (2.0 * bv[A]);
-          else if (fabs(bv[A] - bv[B]) < 1e-9 * (fabs(bv[A]) + fabs(bv[B]) + 1.0)) v = 1.0 / (bv[A] + bv[B]);
-          else v = (lyv[A] - lyv[B]) / (bv[A] - bv[B]);
-          gam[3 * A + B] = v;
+        for (int B = A; B < 3; ++B) {
+          const TT h = Qt[3 * pp + A] * MQ[3 * qq + B] + MQ[3 * qq + A] * Qt[3 * pp + B];
+          const TT v = gam[3 * A + B] * h;
+          Y[3 * A + B] = v;
+          Y[3 * B + A] = v;
         }
-      double MQ[9];   // (Cp Fb^T) Q
-      double NN[9];   // Q^T Fb^-T
-      double FbiT[9];
+      const TT trY = Y[0] + Y[4] + Y[8];
+      const TT nd = nv[0] * Y[0] + nv[1] * Y[4] + nv[2] * Y[8];
+      TT dt[9];
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
+      for (int i = 0; i < 9; ++i) dt[i] = c2 * Y[i];
+      dt[0] += c1 * trY + c3 * nd * nv[0];
+      dt[4] += c1 * trY + c3 * nd * nv[1];
+      dt[8] += c1 * trY + c3 * nd * nv[2];
+      TT T[9];  // dt' N
 #pragma unroll
-        for (int j = 0; j < 3; ++j) FbiT[3 * i + j] = Fbi[3 * j + i];
+      for (int A = 0; A < 3; ++A)
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) T[3 * A + j] = dt[3 * A] * NN[j] + dt[3 * A + 1] * NN[3 + j] + dt[3 * A + 2] * NN[6 + j];
+      const TT Fq = Ft[3 * pp + qq];  // standard F for the F-bar vec(F)
 #pragma unroll
-        for (int B = 0; B < 3; ++B) {
-          MQ[3 * i + B] = M[3 * i] * Q[B] + M[3 * i + 1] * Q[3 + B] + M[3 * i + 2] * Q[6 + B];
-          NN[3 * i + B] = Q[i] * FbiT[B] + Q[3 + i] * FbiT[3 + B] + Q[6 + i] * FbiT[6 + B];
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const TT dP = Qt[3 * i] * T[j] + Qt[3 * i + 1] * T[3 + j] + Qt[3 * i + 2] * T[6 + j] - Pt[3 * i + qq] * FbiT[3 * pp + j];
+          As[(j * 3 + i) * 9 + col] = ws_ * dP;
+          uacc[j * 3 + i] += dP * Fq;
         }
-      // tangent modulus D in principal form:
-      //   dtau' = c2 Y + c1 tr(Y) I + c3 (n . diag Y) diag(n)
-      const double c2 = 2.0 * G - 3.0 * G * b0;
-      const double c1 = lam + G * b0;
-      const double c3 = 3.0 * G * (b0 - g0c);
-      const double nv[3] = {n0, n1, n2};
-      const double ws_ = w * scale;
-      double uacc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-      for (int col = 0; col < 9; ++col) {
-        const int pp = col % 3, qq = col / 3;
-        double Y[9];
-#pragma unroll
-        for (int A = 0; A < 3; ++A)
-#pragma unroll
-          for (int B = A; B < 3; ++B) {
-            const double h = Q[3 * pp + A] * MQ[3 * qq + B] + MQ[3 * qq + A] * Q[3 * pp + B];
-            const double v = gam[3 * A + B] * h;
-            Y[3 * A + B] = v;
-            Y[3 * B + A] = v;
-          }
-        const double trY = Y[0] + Y[4] + Y[8];
-        const double nd = nv[0] * Y[0] + nv[1] * Y[4] + nv[2] * Y[8];
-        double dt[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) dt[i] = c2 * Y[i];
-        dt[0] += c1 * trY + c3 * nd * nv[0];
-        dt[4] += c1 * trY + c3 * nd * nv[1];
-        dt[8] += c1 * trY + c3 * nd * nv[2];
-        double T[9];  // dt' N
-#pragma unroll
-        for (int A = 0; A < 3; ++A)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) T[3 * A + j] = dt[3 * A] * NN[j] + dt[3 * A + 1] * NN[3 + j] + dt[3 * A + 2] * NN[6 + j];
-        const double Fq = F[3 * pp + qq];  // standard F for the F-bar vec(F)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            const double dP = Q[3 * i] * T[j] + Q[3 * i + 1] * T[3 + j] + Q[3 * i + 2] * T[6 + j] - P[3 * i + qq] * FbiT[3 * pp + j];
-            As[(j * 3 + i) * 9 + col] = ws_ * dP;
-            uacc[j * 3 + i] += dP * Fq;
-          }
-      }
-      const double uf = w * scale / 3.0;
-#pragma unroll
-      for (int r = 0; r < 9; ++r) uv[r] = FBAR ? uf * uacc[r] : 0.0;
-      // F^-1 of the standard F = scale * Fb^-1 (for gJ = G^T vec(F^-T))
-#pragma unroll
-      for (int i = 0; i < 9; ++i) Fiu[i] = scale * Fbi[i];
     }
-  }
-  if (COMMIT) return;
-  __syncwarp();
+    const TT uf = (TT)(w * scale / 3.0);
+#pragma unroll
+    for (int r = 0; r < 9; ++r) Rg[105 + r] = FBAR ? uf * uacc[r] : TT(0);
+    // F^-1 of the standard F = scale * Fb^-1 (for gJ = G^T vec(F^-T))
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Rg[114 + i] = (TT)(scale * Fbi[i]);
+    __syncwarp();
 
-  // ---- Phase B: Ke columns, scatter into the block-CSR tangent ----
-  for (int s = 0; s < EPW; ++s) {
-    const long long ls = ((long long)blockIdx.x * WPB + warp) * EPW + s;
-    if (ls >= nlist) break;
-    const int es = elist[ls];
-    const double* Ss = ws + s * SLOT;
-    if (lane < 24) {
-      const int b = lane / 3, k = lane % 3;
-      double acc[24];
-#pragma unroll
-      for (int r = 0; r < 24; ++r) acc[r] = 0.0;
-      const double g0bk = FBAR ? Ss[48 + lane] : 0.0;
+  // ---- Phase B: the warp's 4 x 24 Ke columns over 32 lanes, scatter into
+  // the block-CSR tangent ----
 #pragma unroll 1
-      for (int gg = 0; gg < 8; ++gg) {
-        const double* Rg = Ss + 72 + gg * GPREC;
-        const double* dX = Rg;
-        const double* A = Rg + 24;
-        const double* u = Rg + 105;
-        const double* Fi = Rg + 114;
-        const double db0 = dX[b * 3], db1 = dX[b * 3 + 1], db2 = dX[b * 3 + 2];
-        // dg_(b,k) = g0_(b,k) - gJ_(b,k),  gJ_(b,k) = sum_j F^-1[j][k] dNdX[b][j]
-        const double dgbk = FBAR ? (g0bk - (Fi[k] * db0 + Fi[3 + k] * db1 + Fi[6 + k] * db2)) : 0.0;
-        double T[9];
+  for (int t = lane; t < EPW * 24; t += 32) {
+    const int s = t / 24, col = t - 24 * s;
+    const long long ls = ((long long)blockIdx.x * WPB + warp) * EPW + s;
+    if (ls >= nlist) continue;
+    const int es = elist[ls];
+    const TT* Ss = wbase + s * SLOT_TT;
+    const int b = col / 3, k = col - 3 * b;
+    TT acc[24];
 #pragma unroll
-        for (int r = 0; r < 9; ++r)
-          T[r] = A[r * 9 + k] * db0 + A[r * 9 + 3 + k] * db1 + A[r * 9 + 6 + k] * db2 + u[r] * dgbk;
+    for (int r = 0; r < 24; ++r) acc[r] = TT(0);
+    const TT g0bk = FBAR ? Ss[col] : TT(0);
+#pragma unroll 1
+    for (int gg = 0; gg < 8; ++gg) {
+      const TT* Rr = Ss + 24 + gg * GPREC;
+      const TT* dX = Rr;
+      const TT* A = Rr + 24;
+      const TT* u = Rr + 105;
+      const TT* Fi = Rr + 114;
+      const TT db0 = dX[b * 3], db1 = dX[b * 3 + 1], db2 = dX[b * 3 + 2];
+      // dg_(b,k) = g0_(b,k) - gJ_(b,k),  gJ_(b,k) = sum_j F^-1[j][k] dNdX[b][j]
+      const TT dgbk = FBAR ? (g0bk - (Fi[k] * db0 + Fi[3 + k] * db1 + Fi[6 + k] * db2)) : TT(0);
+      TT T[9];
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const double x0 = dX[a * 3], x1 = dX[a * 3 + 1], x2 = dX[a * 3 + 2];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) acc[a * 3 + i] += x0 * T[i] + x1 * T[3 + i] + x2 * T[6 + i];
-        }
-      }
-      const int* nds = nodes_s[warp][s];
+      for (int r = 0; r < 9; ++r)
+        T[r] = A[r * 9 + k] * db0 + A[r * 9 + 3 + k] * db1 + A[r * 9 + 6 + k] * db2 + u[r] * dgbk;
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
-        const long long blk = (long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b];
-        KT* v = p.Kval + blk * 9 + k;
-        v[0] += (KT)acc[a * 3 + 0];
-        v[3] += (KT)acc[a * 3 + 1];
-        v[6] += (KT)acc[a * 3 + 2];
+        const TT x0 = dX[a * 3], x1 = dX[a * 3 + 1], x2 = dX[a * 3 + 2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) acc[a * 3 + i] += x0 * T[i] + x1 * T[3 + i] + x2 * T[6 + i];
       }
     }
+    const int* nds = nodes_s[warp][s];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const long long blk = (long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b];
+      KT* v = p.Kval + blk * 9 + k;
+      v[0] += (KT)acc[a * 3 + 0];
+      v[3] += (KT)acc[a * 3 + 1];
+      v[6] += (KT)acc[a * 3 + 2];
+    }
   }
+  }  // !COMMIT
 }
 
 template <typename KT, bool COMMIT, bool FBAR>
@@ -464,7 +472,7 @@ static void launch_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_
   if (n <= 0) return;
   const int warps = (n + EPW - 1) / EPW;
   const int blocks = (warps + WPB - 1) / WPB;
-  const size_t sm = (size_t)WPB * WARP_SMEM * sizeof(double);
+  const size_t sm = (size_t)WPB * warp_smem_bytes<KT>(COMMIT);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(element_color_kernel<KT, COMMIT, FBAR>,
@@ -488,7 +496,5 @@ void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool c
 
 template void launch_element_color<double>(const ElemArgs<double>&, const int*, int, bool, bool, cudaStream_t);
 template void launch_element_color<float>(const ElemArgs<float>&, const int*, int, bool, bool, cudaStream_t);
-
-size_t element_smem_bytes() { return (size_t)WPB * WARP_SMEM * sizeof(double); }
 
 }  // namespace pfem

@@ -574,23 +574,39 @@ __global__ void sa_rap_kernel(int nnzC, const int* __restrict__ c_row, const int
     for (int q = 0; q < 6; ++q) O[r * 6 + q] = acc[r][q];
 }
 
-// Restriction bc[I*6+c] = sum_{p in P^T row I} (P_p^T r_row(p))_c
+// Restriction bc = P^T r, one warp per aggregate: the lanes stride over the
+// P blocks of the aggregate's column (the fine rows its smoothed basis
+// reaches) and the six partial sums are combined by a fixed xor tree, so the
+// result is deterministic.
 template <typename T, int BS>
 __global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, const int* __restrict__ pt_blk,
                                    const int* __restrict__ p_row, const T* __restrict__ pval,
                                    const T* __restrict__ r, T* __restrict__ bc) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nagg * 6) return;
-  const int I = (int)(i / 6), c = (int)(i % 6);
-  T s = T(0);
-  for (int t = pt_rp[I]; t < pt_rp[I + 1]; ++t) {
+  const int I = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (I >= nagg) return;  // whole warps exit together
+  T s[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  const int t1 = pt_rp[I + 1];
+  for (int t = pt_rp[I] + lane; t < t1; t += 32) {
     const int p = pt_blk[t];
     const T* P = pval + (long long)p * BS * 6;
     const T* rv = r + (long long)p_row[p] * BS;
 #pragma unroll
-    for (int j = 0; j < BS; ++j) s += P[j * 6 + c] * rv[j];
+    for (int j = 0; j < BS; ++j) {
+      const T rj = rv[j];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) s[c] += P[j * 6 + c] * rj;
+    }
   }
-  bc[i] = s;
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(0xffffffffu, s[c], o);
+  T out = s[0];
+#pragma unroll
+  for (int c = 1; c < 6; ++c)
+    if (lane == c) out = s[c];
+  if (lane < 6) bc[(long long)I * 6 + lane] = out;
 }
 // Prolongation x[n*BS+j] += sum_{p in P row n} (P_p xc[col(p)])_j
 template <typename T, int BS>
@@ -636,7 +652,7 @@ void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t s
 }
 template <typename T>
 void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st) {
-  const long long n = (long long)v.nagg * 6;
+  const long long n = (long long)v.nagg * 32;  // one warp per aggregate
   const int blocks = (int)((n + 255) / 256);
   pfem::count_launch();
   if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_blk, v.p_row, v.p_val, r, bc);

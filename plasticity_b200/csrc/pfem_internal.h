@@ -32,7 +32,6 @@ struct ElemArgs {
 template <typename KT>
 void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit, bool fbar,
                           cudaStream_t st);
-size_t element_smem_bytes();
 
 // ---------------- block-CSR matrices ----------------
 template <typename VT>

@@ -96,11 +96,15 @@ def _check_solve(M, g, prec_label, iters_tol=1):
 
 def _solve_pair(w, g, precision):
     """Newton counts at the case tolerance (FP64, near-exact inner solves, the
-    reference's algorithm) and the converged state at tol 1e-10."""
+    reference's algorithm) and the converged state at tol 1e-10.  The golden
+    counts come from direct solves; the F-bar tangent is nonsymmetric, so the
+    near-exact inner solve here is BiCGStab to 1e-10 (CG on it stalls short of
+    tight tolerances, which makes the counts depend on rounding)."""
     ls = bool(int(g["line_search"]))
     if precision == "fp64":
         M = model_from(w)
-        res = M.solve(nsteps=w.nsteps, tol=float(g["tol"]), maxiter=25, lin_rtol=1e-12, line_search=ls)
+        res = M.solve(nsteps=w.nsteps, tol=float(g["tol"]), maxiter=25, linsolve="bicgstab", lin_rtol=1e-10,
+                      cg_itmax=1000, line_search=ls)
         assert res.converged
         assert np.abs(np.array(res.iters) - g["iters"]).max() <= 1, (res.iters, list(g["iters"]))
     M = model_from(w)
