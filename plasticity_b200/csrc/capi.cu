@@ -41,6 +41,23 @@ struct KrylovWork {
   T *xa = nullptr, *b0 = nullptr;  // iterative refinement: accumulated solution, saved right-hand side
 };
 
+// The preconditioned-CG loop captured as one CUDA graph: a prefix (x = 0,
+// r = b, |b|) and a conditional WHILE node whose body is one iteration
+// (V-cycle, two dot products, the p / x / r updates, |r|) ending in a
+// one-thread kernel that sets the loop condition from the device-resident
+// residual.  One launch and one host synchronisation per linear solve.
+// Re-captured when the AMG hierarchy is rebuilt (its Chebyshev coefficients
+// are kernel arguments); the tolerance and iteration cap are read from ctl.
+struct CgGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t body_stream = nullptr;
+  long long amg_version = -1;
+  double* ctl = nullptr;   // device: [0] rtol, [1] itmax, [2] absolute threshold (set on the device)
+  int* state = nullptr;    // device: [0] iterations, [1] converged
+  long long prefix_kernels = 0, body_kernels = 0;
+};
+
 struct HostLevel {
   int nbrow = 0, bs = 0;
   std::vector<int> rowptr, col;   // matrix pattern of this level
@@ -101,6 +118,7 @@ struct pfem_ctx {
   Amg<double> amg64;
   KrylovWork<float> kw32;
   KrylovWork<double> kw64;
+  CgGraph cg32, cg64;
   int tangent_prec = -1;  // precision of the last imposed tangent
   cudaEvent_t e0 = nullptr, e1 = nullptr, t0 = nullptr, t1 = nullptr;
   // learned predictor
@@ -479,6 +497,12 @@ KrylovWork<float>& kw_of<float>(pfem_ctx* c) { return c->kw32; }
 template <>
 KrylovWork<double>& kw_of<double>(pfem_ctx* c) { return c->kw64; }
 template <typename T>
+CgGraph& cg_of(pfem_ctx* c);
+template <>
+CgGraph& cg_of<float>(pfem_ctx* c) { return c->cg32; }
+template <>
+CgGraph& cg_of<double>(pfem_ctx* c) { return c->cg64; }
+template <typename T>
 T* K_of(pfem_ctx* c);
 template <>
 float* K_of<float>(pfem_ctx* c) { return c->dK32; }
@@ -680,6 +704,7 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     CK(cudaStreamSynchronize(ctx->st));
   }
   A.built = true;
+  A.version++;
   return PFEM_OK;
 }
 
@@ -728,6 +753,123 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
   cheb<T>(ctx, v, A.cheb_degree, b, x, false);
 }
 
+template <typename T>
+__global__ void cg_graph_init_kernel(cudaGraphConditionalHandle h, const T* __restrict__ bn, T* __restrict__ sc0,
+                                     double* __restrict__ ctl, int* __restrict__ state) {
+  const double b = (double)*bn;
+  ctl[2] = ctl[0] * b;
+  state[0] = 0;
+  state[1] = b == 0.0 ? 1 : 0;  // b = 0: x = 0 is the solution
+  *sc0 = T(1);                  // with p = 0, the first update p = z + (r.z / 1) p gives p = z
+  cudaGraphSetConditional(h, (b > 0.0 && isfinite(b)) ? 1u : 0u);
+}
+template <typename T>
+__global__ void cg_graph_check_kernel(cudaGraphConditionalHandle h, const T* __restrict__ rn,
+                                      const double* __restrict__ ctl, int* __restrict__ state) {
+  const int it = state[0] + 1;
+  state[0] = it;
+  const double r = (double)*rn;
+  const bool conv = r <= ctl[2];
+  state[1] = conv ? 1 : 0;
+  cudaGraphSetConditional(h, (!conv && isfinite(r) && it < (int)ctl[1]) ? 1u : 0u);
+}
+
+// Capture (or reuse) the device-side CG loop for the current hierarchy.
+template <typename T>
+int cg_graph_build(pfem_ctx* ctx) {
+  CgGraph& G = cg_of<T>(ctx);
+  Amg<T>& A = amg_of<T>(ctx);
+  if (G.exec && G.amg_version == A.version) return PFEM_OK;
+  if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+  if (G.graph) { cudaGraphDestroy(G.graph); G.graph = nullptr; }
+  if (!G.ctl) {
+    CK(dalloc(ctx, &G.ctl, 4));
+    CK(dalloc(ctx, &G.state, 4));
+    CK(cudaStreamCreateWithFlags(&G.body_stream, cudaStreamNonBlocking));
+  }
+  KrylovWork<T>& w = kw_of<T>(ctx);
+  const BsrMat<T>& K = A.lv[0].A;
+  const long long n = ctx->ndof;
+  cudaStream_t st = ctx->st;
+  const long long c0 = pfem::launch_counter();
+  cudaGraph_t g = nullptr;
+  cudaGraph_t body = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(ctx, PFEM_ERR_CUDA, std::string("CG graph capture: ") + cudaGetErrorString(e));
+  auto abort_capture = [&](cudaError_t err, const char* what) {
+    cudaGraph_t junk = nullptr;
+    ctx->st = st;
+    cudaStreamEndCapture(G.body_stream, &junk);
+    cudaStreamEndCapture(st, &junk);
+    if (junk) cudaGraphDestroy(junk);
+    cudaGetLastError();
+    return fail(ctx, PFEM_ERR_CUDA, std::string("CG graph capture (") + what + "): " + cudaGetErrorString(err));
+  };
+  fill<T>(n, w.x, T(0), st);
+  fill<T>(n, w.p, T(0), st);
+  e = cudaMemcpyAsync(w.r, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return abort_capture(e, "r = b");
+  dot<T>(n, w.b, w.b, w.sc + 10, w.part, st, true);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd);
+  if (e != cudaSuccess) return abort_capture(e, "capture info");
+  cudaGraphConditionalHandle h;
+  e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+  if (e != cudaSuccess) return abort_capture(e, "conditional handle");
+  cg_graph_init_kernel<T><<<1, 1, 0, st>>>(h, w.sc + 10, w.sc + 0, G.ctl, G.state);
+  e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd);
+  if (e != cudaSuccess) return abort_capture(e, "capture info");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  e = cudaGraphAddNode(&cnode, g, deps, nd, &cp);
+  if (e != cudaSuccess) return abort_capture(e, "conditional node");
+  e = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+  if (e != cudaSuccess) return abort_capture(e, "capture dependencies");
+  const long long c1 = pfem::launch_counter();
+  // ---- loop body: one PCG iteration ----
+  body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(G.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return abort_capture(e, "body capture");
+  cudaStream_t bs = G.body_stream;
+  ctx->st = bs;  // the V-cycle launches on ctx->st
+  vcycle<T>(ctx, 0, w.r, w.z);
+  ctx->st = st;
+  dot<T>(n, w.r, w.z, w.sc + 2, w.part, bs, false);
+  cg_p<T>(n, w.sc + 2, w.sc + 0, w.z, w.p, bs);
+  scalar_copy<T>(w.sc + 0, w.sc + 2, bs);
+  bsr_spmv<T>(K, w.p, w.q, bs);
+  dot<T>(n, w.p, w.q, w.sc + 1, w.part, bs, false);
+  cg_xr<T>(n, w.sc + 0, w.sc + 1, w.p, w.q, w.x, w.r, bs);
+  dot<T>(n, w.r, w.r, w.sc + 3, w.part, bs, true);
+  cg_graph_check_kernel<T><<<1, 1, 0, bs>>>(h, w.sc + 3, G.ctl, G.state);
+  e = cudaStreamEndCapture(bs, &body);
+  if (e != cudaSuccess) return abort_capture(e, "body end");
+  const long long c2 = pfem::launch_counter();
+  e = cudaStreamEndCapture(st, &g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, PFEM_ERR_CUDA, std::string("CG graph capture (end): ") + cudaGetErrorString(e));
+  }
+  G.graph = g;
+  e = cudaGraphInstantiate(&G.exec, g, 0);
+  if (e != cudaSuccess) {
+    G.exec = nullptr;
+    return fail(ctx, PFEM_ERR_CUDA, std::string("CG graph instantiate: ") + cudaGetErrorString(e));
+  }
+  // launches are counted when the graph runs, not when it is captured
+  G.prefix_kernels = c1 - c0 + 1;
+  G.body_kernels = c2 - c1 + 1;
+  pfem::launch_counter() = c0;
+  G.amg_version = A.version;
+  return PFEM_OK;
+}
+
 // Preconditioned CG / BiCGStab on level-0 operator with the AMG V-cycle.
 // b and the result x live in kw.b / kw.x.  Returns iterations (>=0) or <0.
 template <typename T>
@@ -739,6 +881,21 @@ int krylov_inner(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, 
   cudaStream_t st = ctx->st;
   *iters = 0;
   *conv = false;
+  if (method == PFEM_KRYLOV_CG) {
+    int rc = cg_graph_build<T>(ctx);
+    if (rc) return rc;
+    CgGraph& G = cg_of<T>(ctx);
+    const double ctl[2] = {rtol, (double)std::max(itmax, 1)};
+    CK(cudaMemcpyAsync(G.ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+    CK(cudaGraphLaunch(G.exec, st));
+    int sh[2] = {0, 0};
+    CK(cudaMemcpyAsync(sh, G.state, sizeof(sh), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *iters = sh[0];
+    *conv = sh[1] != 0;
+    pfem::launch_counter() += G.prefix_kernels + (long long)sh[0] * G.body_kernels;
+    return PFEM_OK;
+  }
   fill<T>(n, w.x, T(0), st);
   CK(cudaMemcpyAsync(w.r, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
   dot<T>(n, w.b, w.b, w.sc + 10, w.part, st, true);
@@ -747,27 +904,7 @@ int krylov_inner(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, 
   CK(cudaStreamSynchronize(st));
   if (!(bn > 0)) { *conv = true; return PFEM_OK; }
   const double thr = rtol * (double)bn;
-  if (method == PFEM_KRYLOV_CG) {
-    vcycle<T>(ctx, 0, w.r, w.z);
-    dot<T>(n, w.r, w.z, w.sc + 0, w.part, st, false);
-    CK(cudaMemcpyAsync(w.p, w.z, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    for (int it = 1; it <= itmax; ++it) {
-      bsr_spmv<T>(K, w.p, w.q, st);
-      dot<T>(n, w.p, w.q, w.sc + 1, w.part, st, false);
-      cg_xr<T>(n, w.sc + 0, w.sc + 1, w.p, w.q, w.x, w.r, st);
-      dot<T>(n, w.r, w.r, w.sc + 3, w.part, st, true);
-      T rn = 0;
-      CK(cudaMemcpyAsync(&rn, w.sc + 3, sizeof(T), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      *iters = it;
-      if ((double)rn <= thr) { *conv = true; break; }
-      if (!std::isfinite((double)rn)) break;
-      vcycle<T>(ctx, 0, w.r, w.z);
-      dot<T>(n, w.r, w.z, w.sc + 2, w.part, st, false);
-      cg_p<T>(n, w.sc + 2, w.sc + 0, w.z, w.p, st);
-      scalar_copy<T>(w.sc + 0, w.sc + 2, st);
-    }
-  } else {
+  {  // BiCGStab: host-driven loop
     CK(cudaMemcpyAsync(w.rh, w.b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
     fill<T>(n, w.v, T(0), st);
     fill<T>(n, w.p, T(0), st);
@@ -1363,6 +1500,11 @@ void pfem_destroy(pfem_ctx* ctx) {
   }
   cudaSetDevice(ctx->device);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
+  for (CgGraph* g : {&ctx->cg32, &ctx->cg64}) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->body_stream) cudaStreamDestroy(g->body_stream);
+  }
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->e0) cudaEventDestroy(ctx->e0);
   if (ctx->e1) cudaEventDestroy(ctx->e1);

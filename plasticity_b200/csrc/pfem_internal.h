@@ -80,6 +80,7 @@ struct Amg {
   VT *cx = nullptr, *cb = nullptr;
   bool built = false;
   int cheb_degree = 2;
+  long long version = 0;     // bumped by every numeric set-up (captured solver graphs key on it)
 };
 
 }  // namespace pfem
