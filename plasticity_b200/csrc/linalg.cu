@@ -20,32 +20,38 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
                                                        const T* __restrict__ x, T* __restrict__ y,
                                                        const T* __restrict__ b,
                                                        const T* __restrict__ dinv, T* __restrict__ xo) {
-  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= nbrow) return;
-  const int s = rowptr[row], e = rowptr[row + 1];
+  // Half a warp per block row (a level-0 row has at most 27 blocks: two per
+  // lane); values and column ids are read once, through the streaming
+  // (evict-first) path so they do not push the gathered x out of the caches.
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4);
+  const int lane = threadIdx.x & 15;
+  const bool ok = row < nbrow;
+  const int s = ok ? rowptr[row] : 0, e = ok ? rowptr[row + 1] : 0;
   T acc[BS];
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
-  for (int k = s + lane; k < e; k += 32) {
-    const int c = col[k];
+  for (int k = s + lane; k < e; k += 16) {
+    const int c = __ldcs(col + k);
     const T* B = val + (long long)k * (BS * BS);
+    T bv[BS * BS];
+#pragma unroll
+    for (int q = 0; q < BS * BS; ++q) bv[q] = __ldcs(B + q);
     T xv[BS];
 #pragma unroll
     for (int j = 0; j < BS; ++j) xv[j] = x[(long long)c * BS + j];
 #pragma unroll
     for (int i = 0; i < BS; ++i)
 #pragma unroll
-      for (int j = 0; j < BS; ++j) acc[i] += B[i * BS + j] * xv[j];
+      for (int j = 0; j < BS; ++j) acc[i] += bv[i * BS + j] * xv[j];
   }
 #pragma unroll
   for (int i = 0; i < BS; ++i) {
     T v = acc[i];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     acc[i] = v;
   }
-  if (lane < BS) {
+  if (ok && lane < BS) {
     const long long base = (long long)row * BS;
     T v = acc[0];
 #pragma unroll
@@ -69,7 +75,7 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
 
 template <typename T>
 void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 32;
+  const long long threads = (long long)A.nbrow * 16;
   const int blocks = (int)((threads + 255) / 256);
   pfem::count_launch();
   if (A.bs == 3)
@@ -79,7 +85,7 @@ void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st) {
 }
 template <typename T>
 void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 32;
+  const long long threads = (long long)A.nbrow * 16;
   const int blocks = (int)((threads + 255) / 256);
   pfem::count_launch();
   if (A.bs == 3)
@@ -89,7 +95,7 @@ void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t
 }
 template <typename T>
 void bsr_cheb_step(const BsrMat<T>& A, const T* dinv, const T* d, T* r, T* x, cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 32;
+  const long long threads = (long long)A.nbrow * 16;
   const int blocks = (int)((threads + 255) / 256);
   pfem::count_launch();
   if (A.bs == 3)
@@ -595,7 +601,7 @@ __global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, cons
     for (int j = 0; j < BS; ++j) {
       const T rj = rv[j];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) s[c] += P[j * 6 + c] * rj;
+      for (int c = 0; c < 6; ++c) s[c] += __ldcs(P + j * 6 + c) * rj;
     }
   }
 #pragma unroll
@@ -620,7 +626,7 @@ __global__ void sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp, const
     const T* P = pval + (long long)p * BS * 6 + j * 6;
     const T* xa = xc + (long long)p_cl[p] * 6;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) s += P[c] * xa[c];
+    for (int c = 0; c < 6; ++c) s += __ldcs(P + c) * xa[c];
   }
   x[i] += s;
 }
