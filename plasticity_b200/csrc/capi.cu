@@ -718,6 +718,17 @@ void cheb(pfem_ctx* ctx, AmgLevel<T>& v, int degree, const T* b, T* x, bool zero
   const double th = 0.5 * (lmx + lmn), de = 0.5 * (lmx - lmn);
   const double sg = th / de;
   double rho = 1.0 / sg;
+  if (degree == 2) {
+    // x2 = x0 + d0 + d1 with d0 = r0 / th, r0 = Dinv (b - A x0), r1 = r0 - Dinv A d0,
+    // d1 = (2 rn / de) r1 + rn rho d0: one block-Jacobi pass (or a fused
+    // residual pass) and one fused SpMV pass.
+    const double rn = 1.0 / (2.0 * sg - rho);
+    const T c1 = T(2.0 * rn / de), c2 = T(1.0 + rn * rho);
+    if (zero) blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, b, v.r, T(1.0 / th), v.d, ctx->st);
+    else bsr_residual_precond<T>(v.A, v.dinv, x, b, v.r, v.d, T(1.0 / th), ctx->st);
+    bsr_cheb2<T>(v.A, v.dinv, v.d, v.r, x, zero, c1, c2, ctx->st);
+    return;
+  }
   if (zero) {
     fill<T>(n, x, T(0), ctx->st);
     blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, b, v.r, T(1.0 / th), v.d, ctx->st);

@@ -19,7 +19,8 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
                                                        const T* __restrict__ val,
                                                        const T* __restrict__ x, T* __restrict__ y,
                                                        const T* __restrict__ b,
-                                                       const T* __restrict__ dinv, T* __restrict__ xo) {
+                                                       const T* __restrict__ dinv, T* __restrict__ xo,
+                                                       T c1, T c2) {
   // Half a warp per block row (a level-0 row has at most 27 blocks: two per
   // lane); values and column ids are read once, through the streaming
   // (evict-first) path so they do not push the gathered x out of the caches.
@@ -53,6 +54,16 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
   }
   if (ok && lane < BS) {
     const long long base = (long long)row * BS;
+    if (MODE == 5) {
+      // r = Dinv (b - A x) (into y), d = c1 r (into xo)
+      const T* D = dinv + (long long)row * (BS * BS);
+      T t = T(0);
+#pragma unroll
+      for (int j = 0; j < BS; ++j) t += D[lane * BS + j] * (b[base + j] - acc[j]);
+      y[base + lane] = t;
+      xo[base + lane] = c1 * t;
+      return;
+    }
     T v = acc[0];
 #pragma unroll
     for (int i = 1; i < BS; ++i)
@@ -62,46 +73,59 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
     } else if (MODE == 1) {
       y[base + lane] = b[base + lane] - v;
     } else {
-      // r_i -= Dinv_i (A d)_i  (row lane of the bs x bs block product)
+      // t = (Dinv A d)_lane with d = x (the gathered vector)
       const T* D = dinv + (long long)row * (BS * BS);
       T t = T(0);
 #pragma unroll
       for (int j = 0; j < BS; ++j) t += D[lane * BS + j] * acc[j];
-      y[base + lane] -= t;
-      xo[base + lane] += x[base + lane];
+      if (MODE == 2) {
+        y[base + lane] -= t;
+        xo[base + lane] += x[base + lane];
+      } else {
+        // degree-2 Chebyshev in one pass: r1 = r0 - Dinv A d0,
+        // x2 = x0 + c2 d0 + c1 r1 (c2 = 1 + rn rho, c1 = 2 rn / delta)
+        const T upd = c2 * x[base + lane] + c1 * (y[base + lane] - t);
+        if (MODE == 3) xo[base + lane] = upd;
+        else xo[base + lane] += upd;
+      }
     }
   }
 }
 
-template <typename T>
-void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st) {
+template <typename T, int MODE>
+static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const T* dinv, T* xo, T c1, T c2,
+                        cudaStream_t st) {
   const long long threads = (long long)A.nbrow * 16;
   const int blocks = (int)((threads + 255) / 256);
   pfem::count_launch();
   if (A.bs == 3)
-    bsr_spmv_kernel<T, 3, 0><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, nullptr, nullptr, nullptr);
+    bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
   else
-    bsr_spmv_kernel<T, 6, 0><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, nullptr, nullptr, nullptr);
+    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+}
+
+template <typename T>
+void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st) {
+  spmv_launch<T, 0>(A, x, y, nullptr, nullptr, nullptr, T(0), T(0), st);
 }
 template <typename T>
 void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 16;
-  const int blocks = (int)((threads + 255) / 256);
-  pfem::count_launch();
-  if (A.bs == 3)
-    bsr_spmv_kernel<T, 3, 1><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, r, b, nullptr, nullptr);
-  else
-    bsr_spmv_kernel<T, 6, 1><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, r, b, nullptr, nullptr);
+  spmv_launch<T, 1>(A, x, r, b, nullptr, nullptr, T(0), T(0), st);
 }
 template <typename T>
 void bsr_cheb_step(const BsrMat<T>& A, const T* dinv, const T* d, T* r, T* x, cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 16;
-  const int blocks = (int)((threads + 255) / 256);
-  pfem::count_launch();
-  if (A.bs == 3)
-    bsr_spmv_kernel<T, 3, 2><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, d, r, nullptr, dinv, x);
-  else
-    bsr_spmv_kernel<T, 6, 2><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, d, r, nullptr, dinv, x);
+  spmv_launch<T, 2>(A, d, r, nullptr, dinv, x, T(0), T(0), st);
+}
+template <typename T>
+void bsr_cheb2(const BsrMat<T>& A, const T* dinv, const T* d0, const T* r0, T* x, bool zero, T c1, T c2,
+               cudaStream_t st) {
+  if (zero) spmv_launch<T, 3>(A, d0, const_cast<T*>(r0), nullptr, dinv, x, c1, c2, st);
+  else spmv_launch<T, 4>(A, d0, const_cast<T*>(r0), nullptr, dinv, x, c1, c2, st);
+}
+template <typename T>
+void bsr_residual_precond(const BsrMat<T>& A, const T* dinv, const T* x, const T* b, T* r, T* d, T scale,
+                          cudaStream_t st) {
+  spmv_launch<T, 5>(A, x, r, b, dinv, d, scale, T(0), st);
 }
 
 // ------------------------------------------------------------------ block diagonal
@@ -678,6 +702,9 @@ void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
   template void bsr_spmv<T>(const BsrMat<T>&, const T*, T*, cudaStream_t);                         \
   template void bsr_residual<T>(const BsrMat<T>&, const T*, const T*, T*, cudaStream_t);           \
   template void bsr_cheb_step<T>(const BsrMat<T>&, const T*, const T*, T*, T*, cudaStream_t);      \
+  template void bsr_cheb2<T>(const BsrMat<T>&, const T*, const T*, const T*, T*, bool, T, T, cudaStream_t); \
+  template void bsr_residual_precond<T>(const BsrMat<T>&, const T*, const T*, const T*, T*, T*, T,    \
+                                        cudaStream_t);                                             \
   template void blockdiag_apply<T>(int, int, const T*, const T*, T*, T, T*, cudaStream_t);         \
   template void blockdiag_invert<T>(const BsrMat<T>&, T*, cudaStream_t);                           \
   template void dot<T>(long long, const T*, const T*, T*, T*, cudaStream_t, bool);                 \

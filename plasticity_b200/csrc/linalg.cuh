@@ -26,6 +26,12 @@ struct BcDev {
 template <typename T> void bsr_spmv(const BsrMat<T>& A, const T* x, T* y, cudaStream_t st);
 template <typename T> void bsr_residual(const BsrMat<T>& A, const T* x, const T* b, T* r, cudaStream_t st);
 template <typename T> void bsr_cheb_step(const BsrMat<T>& A, const T* dinv, const T* d, T* r, T* x, cudaStream_t st);
+// Degree-2 Chebyshev in one pass: x (=, or += unless zero) c2 d0 + c1 (r0 - Dinv A d0).
+template <typename T> void bsr_cheb2(const BsrMat<T>& A, const T* dinv, const T* d0, const T* r0, T* x, bool zero,
+                                     T c1, T c2, cudaStream_t st);
+// r = Dinv (b - A x), d = scale r.
+template <typename T> void bsr_residual_precond(const BsrMat<T>& A, const T* dinv, const T* x, const T* b, T* r,
+                                                T* d, T scale, cudaStream_t st);
 template <typename T> void blockdiag_apply(int nbrow, int bs, const T* dinv, const T* v, T* r, T scale, T* d, cudaStream_t st);
 template <typename T> void blockdiag_invert(const BsrMat<T>& A, T* dinv, cudaStream_t st);
 template <typename T> void dot(long long n, const T* a, const T* b, T* out, T* part, cudaStream_t st, bool take_sqrt);
