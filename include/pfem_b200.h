@@ -173,8 +173,9 @@ int pfem_residual(pfem_ctx* ctx, double lambda, int32_t precision, double* rnorm
 int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, int32_t rebuild_pc,
                       const pfem_solve_opts* o, int32_t* niter);
 
-/* One V-cycle of the AMG hierarchy last built by pfem_linear_solve / Newton
- * (precision of the resident tangent): z = M^-1 r, host vectors of ndof. */
+/* One cycle of the AMG hierarchy last built by pfem_linear_solve / Newton
+ * (precision of the resident tangent; a V on the finest level, a W below
+ * it): z = M^-1 r, host vectors of ndof. */
 int pfem_amg_apply(pfem_ctx* ctx, const double* r, double* z);
 
 /* Inspection of the resident AMG hierarchy (small problems): the dense

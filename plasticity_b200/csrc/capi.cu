@@ -761,6 +761,15 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
   if (l + 1 < L) vcycle<T>(ctx, l + 1, bn, xn);
   else dense_mv<T>(A.coarse_n, A.coarse_inv, bn, xn, ctx->st);
   sa_prolong<T>(v, xn, x, ctx->st);
+  if (l >= 1 && l + 1 < L) {
+    // Below the finest level the cycle is a W: a second coarse correction
+    // from the updated residual.  The coarse levels cost a small fraction of
+    // level 0, and the stronger coarse solve cuts the outer CG iterations.
+    bsr_residual<T>(v.A, x, b, v.t, ctx->st);
+    sa_restrict<T>(v, v.t, bn, ctx->st);
+    vcycle<T>(ctx, l + 1, bn, xn);
+    sa_prolong<T>(v, xn, x, ctx->st);
+  }
   cheb<T>(ctx, v, A.cheb_degree, b, x, false);
 }
 

@@ -249,7 +249,7 @@ class Model:
 
     def _opts(self, nsteps=10, tol=1e-8, maxiter=25, precision="fp64", linsolve="cg", lin_rtol=None,
               predictor="previous", amg_rebuild=False, cheb_degree=2, cg_itmax=200, eta_min=None,
-              line_search=False, verbose=False, predictor_smooth=None):
+              line_search=False, verbose=False, predictor_smooth=None, eta_max=None):
         o = L.SolveOpts()
         L.lib().pfem_default_opts(C.byref(o))
         o.nsteps, o.maxiter, o.tol = nsteps, maxiter, tol
@@ -268,6 +268,8 @@ class Model:
         o.line_search = int(bool(line_search))
         if predictor_smooth is not None:
             o.predictor_smooth = int(predictor_smooth)
+        if eta_max is not None:
+            o.eta_max = float(eta_max)
         return o
 
     def solve(self, nsteps=10, tol=1e-8, maxiter=25, **kw) -> SolveResult:
@@ -332,7 +334,7 @@ class Model:
         return x, n.value
 
     def amg_apply(self, r):
-        """One V-cycle of the resident AMG hierarchy: z = M^-1 r."""
+        """One cycle of the resident AMG hierarchy (V on level 0, W below): z = M^-1 r."""
         r = np.ascontiguousarray(r, np.float64)
         z = np.zeros(self.ndof)
         check(L.lib().pfem_amg_apply(self._ctx, ptr(r), ptr(z)), self._ctx)

@@ -8,7 +8,10 @@ default), sets a displacement that drives most Gauss points plastic (uniform
   2. the FP64 assembly `reps` times,
   3. the level-0 FP32 block-CSR SpMV on that tangent `reps` times,
   4. the predictor network's forward pass over one row per node `reps` times
-     (weights from plasticity_b200/weights when present, else random).
+     (weights from plasticity_b200/weights when present, else random),
+  5. two AMG set-ups and `reps` AMG-preconditioned CG solves (relative
+     tolerance 1e-4, the device-side CG graph) on the imposed mixed-precision
+     tangent at that displacement.
 
 Each family is timed with CUDA events on the library's stream and printed as one
 JSON line, so the same command serves a launch list, a single-kernel capture
@@ -60,6 +63,16 @@ def main():
     for _ in range(args.reps):
         M.mlp_forward(F)
     out["mlp_forward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    _, R = M.residual(0.05, precision="mixed")
+    M.linear_solve(-R, rtol=1e-4, rebuild=True, precision="mixed")  # symbolic hierarchy, once
+    t0 = time.perf_counter()
+    x, its = M.linear_solve(-R, rtol=1e-4, rebuild=True, precision="mixed")
+    out["amg_setup_and_solve_ms"] = (time.perf_counter() - t0) * 1e3
+    out["cg_iters"] = its
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed")
+    out["cg_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
     print(json.dumps(out), flush=True)
 
 
