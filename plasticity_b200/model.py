@@ -159,6 +159,16 @@ class Model:
         self.neu_dofs, self.neu_vals = [], []
         self._bcs_dirty = True
 
+    _BC_FIELDS = frozenset(("dir_dofs", "dir_vals", "dir_ramp", "neu_dofs", "neu_vals"))
+
+    def __setattr__(self, name, value):
+        # Replacing a boundary-condition list (as Workload.apply does) must
+        # reach the device before the next solve, like the fix!/prescribe!/load!
+        # builders do (Model.jl:102-145; frozen by _freeze_bcs, Solver.jl:192-218).
+        object.__setattr__(self, name, value)
+        if name in Model._BC_FIELDS:
+            object.__setattr__(self, "_bcs_dirty", True)
+
     def __del__(self):
         ctx = getattr(self, "_ctx", None)
         if ctx is not None and ctx.value:

@@ -1,17 +1,19 @@
 """Learned per-node Newton predictor: data generation, training, evaluation.
 
 Training data are converged load increments the solver itself produces on
-32^3 cubes whose top face follows seed-drawn affine motions (combined
-tension/shear/bending, 6 components uniform in +-5% of the size, 20
-increments); the network (12 -> 128 -> 128 -> 3, GELU) learns the correction
+512 load paths of 32^3 cubes whose top face follows seed-drawn affine motions
+(combined tension/shear/bending, 6 components uniform in +-5% of the size,
+20 increments -- every fourth path 40, so the load-step-size input varies);
+the network (12 -> 128 -> 128 -> 3, GELU) learns the correction
 to linear extrapolation of the nodal increment, and is trained on the GPU by the
 library's own forward/backward/Adam kernels (BF16 tensor cores, FP32
 accumulation).  Evaluation runs held-out paths at 64^3 with the extrapolation
 predictor and with the learned one (which falls back to extrapolation whenever
 its guess has the larger FP64 residual).
 
-    python -m plasticity_b200.predictor train --paths 64 --steps 3000 --out plasticity_b200/weights/predictor_mlp.npz
-    python -m plasticity_b200.predictor evaluate --n 64 --paths 8
+    python -m plasticity_b200.predictor train --paths 512 --steps 12000 --out plasticity_b200/weights/predictor_mlp.npz
+    python -m plasticity_b200.predictor evaluate --n 64 --paths 64
+    python -m plasticity_b200.predictor guess --n 32 --paths 4 --smooth 16
 """
 from __future__ import annotations
 
@@ -88,7 +90,7 @@ def guess_errors(M, w, smooth=None, precision="mixed", tol=1e-10):
     return rows
 
 
-def generate(M, n, paths, seed0=1000, nsteps=(20, 40)):
+def generate(M, n, paths, seed0=1000, nsteps=(20, 20, 20, 40)):
     """Record training pairs from `paths` solver-generated load paths; path i
     takes nsteps[i % len(nsteps)] increments, so the load-step-size input
     varies across the set."""
@@ -114,8 +116,8 @@ def main():
     ap.add_argument("cmd", choices=["train", "evaluate", "guess"])
     ap.add_argument("--smooth", type=int, default=None)
     ap.add_argument("--n", type=int, default=32)
-    ap.add_argument("--paths", type=int, default=64)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--paths", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=WEIGHTS)

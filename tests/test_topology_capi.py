@@ -110,3 +110,20 @@ def test_workload_shapes():
     assert (w1.sigy0_e < 250).sum() == 4
     w3 = W.config3(n=12, patch=4)
     assert (w3.dir_vals < 0).sum() == 16
+
+
+def test_boundary_condition_changes_mark_model_dirty():
+    """Re-applying a different load path's BCs to a reused model must be pushed
+    to the device before the next solve."""
+    w1 = W.config4_path(n=3, seed=1)
+    w2 = W.config4_path(n=3, seed=2)
+    M = P.Model(w1.mesh, P.J2Material(**w1.material), device=-1)
+    w1.apply(M)
+    assert M._bcs_dirty
+    M._bcs_dirty = False          # as after a push
+    w2.apply(M)
+    assert M._bcs_dirty
+    assert not np.allclose(w1.dir_vals, w2.dir_vals)
+    M._bcs_dirty = False
+    M.prescribe([1], "x", 0.1)
+    assert M._bcs_dirty
