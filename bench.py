@@ -96,6 +96,19 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def ncu_traffic(kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel`
+    from the committed ncu summary profiles/ncu_traffic.txt, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 2 and not line.startswith("#") and f[0] == kernel:
+            return float(f[1])
+    return None
+
+
 def spmv_bytes(nnzb, nbrow, bs, vbytes):
     """Algorithmic bytes of one block-CSR SpMV: values + block column ids +
     row pointers + x read once + y written once."""
@@ -258,7 +271,8 @@ def main():
     roof = {"kernel": "bsr_spmv_kernel<float,3> (level-0 tangent SpMV, FP32 values)", "bound": "hbm",
             "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
             "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)" if pk_kind == "measured" else pk_kind,
-            "algorithmic_bytes_per_launch": by, "avg_launch_ms": spmv_ms, "traffic": None,
+            "algorithmic_bytes_per_launch": by, "avg_launch_ms": spmv_ms,
+            "traffic": ncu_traffic("bsr_spmv_kernel<float,3,0>"),
             "element_assembly_ms": asm_ms}
     del M
 

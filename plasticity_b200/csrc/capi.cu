@@ -580,6 +580,9 @@ int amg_alloc(pfem_ctx* ctx) {
   A.coarse_nnzb = hc.rowptr[hc.nbrow];
   CK(dalloc(ctx, &A.coarse_val, (size_t)A.coarse_nnzb * 36));
   CK(dalloc(ctx, &A.coarse_inv, (size_t)A.coarse_n * A.coarse_n));
+  CK(upload(ctx, &A.c_rowptr, hc.rowptr));
+  CK(upload(ctx, &A.c_col, hc.col));
+  CK(dalloc(ctx, &A.cwork, (size_t)2 * A.coarse_n * A.coarse_n));
   CK(dalloc(ctx, &A.cx, (size_t)A.coarse_n));
   CK(dalloc(ctx, &A.cb, (size_t)A.coarse_n));
   return PFEM_OK;
@@ -598,39 +601,6 @@ int krylov_alloc(pfem_ctx* ctx) {
   CK(dalloc(ctx, &w.xa, n)); CK(dalloc(ctx, &w.b0, n));
   CK(dalloc(ctx, &w.sc, 16)); CK(dalloc(ctx, &w.part, 2048));
   return PFEM_OK;
-}
-
-// Gauss-Jordan inverse of a dense n x n matrix (row-major, double) with
-// partial pivoting; near-singular pivots are regularised.
-void dense_inverse(int n, std::vector<double>& a, std::vector<double>& inv) {
-  inv.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
-  double scl = 0;
-  for (int i = 0; i < n; ++i) scl = std::max(scl, std::fabs(a[(size_t)i * n + i]));
-  for (int c = 0; c < n; ++c) {
-    int piv = c;
-    double best = std::fabs(a[(size_t)c * n + c]);
-    for (int r = c + 1; r < n; ++r)
-      if (std::fabs(a[(size_t)r * n + c]) > best) { best = std::fabs(a[(size_t)r * n + c]); piv = r; }
-    if (piv != c)
-      for (int j = 0; j < n; ++j) {
-        std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
-        std::swap(inv[(size_t)c * n + j], inv[(size_t)piv * n + j]);
-      }
-    double pv = a[(size_t)c * n + c];
-    if (std::fabs(pv) < 1e-14 * std::max(scl, 1e-300)) pv = (pv >= 0 ? 1.0 : -1.0) * 1e-14 * std::max(scl, 1e-300);
-    const double ip = 1.0 / pv;
-    for (int j = 0; j < n; ++j) { a[(size_t)c * n + j] *= ip; inv[(size_t)c * n + j] *= ip; }
-    for (int r = 0; r < n; ++r) {
-      if (r == c) continue;
-      const double f = a[(size_t)r * n + c];
-      if (f == 0.0) continue;
-      for (int j = 0; j < n; ++j) {
-        a[(size_t)r * n + j] -= f * a[(size_t)c * n + j];
-        inv[(size_t)r * n + j] -= f * inv[(size_t)c * n + j];
-      }
-    }
-  }
 }
 
 // Numeric AMG set-up on the current (Dirichlet-imposed) tangent of precision T:
@@ -678,30 +648,12 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     sa_setup_level<T>(v, omega, cval, nnzC, ctx->st);
     CKL();
   }
-  // coarsest operator: dense inverse on the host (a few hundred dofs)
+  // coarsest operator (a few hundred dofs): dense inverse on the device
   {
     const HostLevel& hc = ctx->hl[L];
-    std::vector<T> hv((size_t)A.coarse_nnzb * 36);
-    CK(cudaMemcpyAsync(hv.data(), A.coarse_val, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    const int n = A.coarse_n;
-    std::vector<double> dense((size_t)n * n, 0.0), inv;
-    for (int I = 0; I < hc.nbrow; ++I)
-      for (int k = hc.rowptr[I]; k < hc.rowptr[I + 1]; ++k) {
-        const int J = hc.col[k];
-        for (int r = 0; r < 6; ++r)
-          for (int c = 0; c < 6; ++c) dense[(size_t)(I * 6 + r) * n + J * 6 + c] = (double)hv[(size_t)k * 36 + r * 6 + c];
-      }
-    // rigid modes absent from an aggregate leave zero rows: put 1 on their diagonal
-    for (int i = 0; i < n; ++i) {
-      bool zero = true;
-      for (int j = 0; j < n && zero; ++j) zero = dense[(size_t)i * n + j] == 0.0;
-      if (zero) dense[(size_t)i * n + i] = 1.0;
-    }
-    dense_inverse(n, dense, inv);
-    std::vector<T> invT(inv.begin(), inv.end());
-    CK(cudaMemcpyAsync(A.coarse_inv, invT.data(), invT.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    coarse_inverse<T>(hc.nbrow, A.c_rowptr, A.c_col, A.coarse_nnzb, A.coarse_val, A.coarse_n, A.cwork,
+                      A.coarse_inv, ctx->st);
+    CKL();
   }
   A.built = true;
   A.version++;

@@ -52,7 +52,7 @@ def run_path(M, w, predictor, precision="mixed", tol=1e-8):
     """Solve one load path on an existing model with the path's BCs; returns stats."""
     w.apply(M)
     t0 = time.perf_counter()
-    r = M.solve(nsteps=w.nsteps, tol=tol, maxiter=40, precision=precision, predictor=predictor,
+    r = M.solve(nsteps=w.nsteps, tol=tol, maxiter=60, precision=precision, predictor=predictor,
                 line_search=True)
     sec = time.perf_counter() - t0
     return dict(converged=r.converged, newton=list(r.iters), krylov=[int(sum(k)) for k in r.cg_iters],
@@ -70,17 +70,22 @@ def guess_errors(M, w, smooth=None, precision="mixed", tol=1e-10):
     M.reset()
     rows = []
     U_prev = np.zeros(M.ndof)
-    kw = dict(precision=precision, line_search=True, tol=tol, maxiter=40)
+    kw = dict(precision=precision, line_search=True, tol=tol, maxiter=60)
     sm = {} if smooth is None else dict(predictor_smooth=smooth)
+    from ._lib import PfemError
     for s in range(1, w.nsteps + 1):
         lam = s / w.nsteps
-        if s <= 2:
-            M.newton(lam, predictor="extrapolate", **kw)
-            U_prev = M.U
-            continue
-        U_ex, _, _, _ = M.predict(lam, "extrapolate", precision=precision)
-        U_ml, r_ex, r_ml, used = M.predict(lam, "learned", precision=precision, **sm)
-        h, k = M.newton(lam, predictor="previous", **kw)
+        try:
+            if s <= 2:
+                M.newton(lam, predictor="extrapolate", **kw)
+                U_prev = M.U
+                continue
+            U_ex, _, _, _ = M.predict(lam, "extrapolate", precision=precision)
+            U_ml, r_ex, r_ml, used = M.predict(lam, "learned", precision=precision, **sm)
+            h, k = M.newton(lam, predictor="previous", **kw)
+        except PfemError as e:  # a load step that does not converge ends the path
+            rows.append(dict(step=s, failed=str(e)))
+            break
         U = M.U
         inc = max(np.linalg.norm(U - U_prev), 1e-300)
         rows.append(dict(step=s, r_extrap=r_ex, r_learned=r_ml, used=used, newton=len(h), krylov=int(sum(k)),
@@ -140,11 +145,13 @@ def main():
     elif args.cmd == "guess":
         M = _path_model(args.n)
         load_into(M, args.out)
-        allr = []
+        allr, failed = [], 0
         for i in range(args.paths):
-            allr += guess_errors(M, W.config4_path(n=args.n, seed=args.seed0 + i), args.smooth)
+            rows = guess_errors(M, W.config4_path(n=args.n, seed=args.seed0 + i), args.smooth)
+            failed += sum("failed" in r for r in rows)
+            allr += [r for r in rows if "failed" not in r]
         med = lambda k: float(np.median([r[k] for r in allr]))
-        print(json.dumps(dict(n=args.n, paths=args.paths, smooth=args.smooth, steps=len(allr),
+        print(json.dumps(dict(n=args.n, paths=args.paths, smooth=args.smooth, steps=len(allr), failed_paths=failed,
                               learned_kept=int(sum(r["used"] for r in allr)),
                               median_err_extrap=med("err_extrap"), median_err_chosen=med("err_chosen"),
                               median_r_extrap=med("r_extrap"), median_r_learned=med("r_learned"),
