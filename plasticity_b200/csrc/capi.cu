@@ -80,6 +80,7 @@ struct pfem_ctx {
   MatParams mat{};
   std::string err;
   std::vector<void*> allocs;
+  std::vector<int> bc_dofs;    // deduplicated Dirichlet dofs of the last pfem_set_bcs
 
   // host topology
   std::vector<double> X;        // nn*3
@@ -168,6 +169,16 @@ cudaError_t upload(pfem_ctx* ctx, T** p, const std::vector<T>& h) {
   if (e != cudaSuccess) return e;
   if (!h.empty()) e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
   return e;
+}
+
+// Free one allocation made by dalloc/upload (nullptr is a no-op).
+template <typename T>
+void dfree(pfem_ctx* ctx, T*& p) {
+  if (!p) return;
+  auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), (void*)p);
+  if (it != ctx->allocs.end()) ctx->allocs.erase(it);
+  cudaFree((void*)p);
+  p = nullptr;
 }
 
 template <class Fn>
@@ -580,9 +591,6 @@ int amg_alloc(pfem_ctx* ctx) {
   A.coarse_nnzb = hc.rowptr[hc.nbrow];
   CK(dalloc(ctx, &A.coarse_val, (size_t)A.coarse_nnzb * 36));
   CK(dalloc(ctx, &A.coarse_inv, (size_t)A.coarse_n * A.coarse_n));
-  CK(upload(ctx, &A.c_rowptr, hc.rowptr));
-  CK(upload(ctx, &A.c_col, hc.col));
-  CK(dalloc(ctx, &A.cwork, (size_t)2 * A.coarse_n * A.coarse_n));
   CK(dalloc(ctx, &A.cx, (size_t)A.coarse_n));
   CK(dalloc(ctx, &A.cb, (size_t)A.coarse_n));
   return PFEM_OK;
@@ -601,6 +609,39 @@ int krylov_alloc(pfem_ctx* ctx) {
   CK(dalloc(ctx, &w.xa, n)); CK(dalloc(ctx, &w.b0, n));
   CK(dalloc(ctx, &w.sc, 16)); CK(dalloc(ctx, &w.part, 2048));
   return PFEM_OK;
+}
+
+// Gauss-Jordan inverse of a dense n x n matrix (row-major, double) with
+// partial pivoting; near-singular pivots are regularised.
+void dense_inverse(int n, std::vector<double>& a, std::vector<double>& inv) {
+  inv.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+  double scl = 0;
+  for (int i = 0; i < n; ++i) scl = std::max(scl, std::fabs(a[(size_t)i * n + i]));
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    double best = std::fabs(a[(size_t)c * n + c]);
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(a[(size_t)r * n + c]) > best) { best = std::fabs(a[(size_t)r * n + c]); piv = r; }
+    if (piv != c)
+      for (int j = 0; j < n; ++j) {
+        std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
+        std::swap(inv[(size_t)c * n + j], inv[(size_t)piv * n + j]);
+      }
+    double pv = a[(size_t)c * n + c];
+    if (std::fabs(pv) < 1e-14 * std::max(scl, 1e-300)) pv = (pv >= 0 ? 1.0 : -1.0) * 1e-14 * std::max(scl, 1e-300);
+    const double ip = 1.0 / pv;
+    for (int j = 0; j < n; ++j) { a[(size_t)c * n + j] *= ip; inv[(size_t)c * n + j] *= ip; }
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      const double f = a[(size_t)r * n + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) {
+        a[(size_t)r * n + j] -= f * a[(size_t)c * n + j];
+        inv[(size_t)r * n + j] -= f * inv[(size_t)c * n + j];
+      }
+    }
+  }
 }
 
 // Numeric AMG set-up on the current (Dirichlet-imposed) tangent of precision T:
@@ -648,12 +689,30 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     sa_setup_level<T>(v, omega, cval, nnzC, ctx->st);
     CKL();
   }
-  // coarsest operator (a few hundred dofs): dense inverse on the device
+  // coarsest operator: dense inverse on the host (a few hundred dofs)
   {
     const HostLevel& hc = ctx->hl[L];
-    coarse_inverse<T>(hc.nbrow, A.c_rowptr, A.c_col, A.coarse_nnzb, A.coarse_val, A.coarse_n, A.cwork,
-                      A.coarse_inv, ctx->st);
-    CKL();
+    std::vector<T> hv((size_t)A.coarse_nnzb * 36);
+    CK(cudaMemcpyAsync(hv.data(), A.coarse_val, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const int n = A.coarse_n;
+    std::vector<double> dense((size_t)n * n, 0.0), inv;
+    for (int I = 0; I < hc.nbrow; ++I)
+      for (int k = hc.rowptr[I]; k < hc.rowptr[I + 1]; ++k) {
+        const int J = hc.col[k];
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 6; ++c) dense[(size_t)(I * 6 + r) * n + J * 6 + c] = (double)hv[(size_t)k * 36 + r * 6 + c];
+      }
+    // rigid modes absent from an aggregate leave zero rows: put 1 on their diagonal
+    for (int i = 0; i < n; ++i) {
+      bool zero = true;
+      for (int j = 0; j < n && zero; ++j) zero = dense[(size_t)i * n + j] == 0.0;
+      if (zero) dense[(size_t)i * n + i] = 1.0;
+    }
+    dense_inverse(n, dense, inv);
+    std::vector<T> invT(inv.begin(), inv.end());
+    CK(cudaMemcpyAsync(A.coarse_inv, invT.data(), invT.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
   }
   A.built = true;
   A.version++;
@@ -1564,6 +1623,15 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   double s = 0;
   for (double v : fn) s += v * v;
   ctx->fn_norm = std::sqrt(s);
+  BcDev& b = ctx->bc;
+  if (ctx->bcs_set && dofs == ctx->bc_dofs) {
+    // same constrained dofs: the imposition lists stand, only values change
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(b.vals, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.ramp, ramp.data(), ramp.size() * sizeof(uint8_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.fn, fn.data(), fn.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return PFEM_OK;
+  }
   // entries touched by the imposition
   auto blk = [&](int n, int m) -> long long {
     const int* b0 = ctx->bcol.data() + ctx->browptr[n];
@@ -1605,7 +1673,8 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   rptr.push_back((int)rpos.size());
   if (rows.empty()) rptr.assign(1, 0);
   for (auto& z : zl) { zpos.push_back(z.first); zone.push_back(z.second); }
-  BcDev& b = ctx->bc;
+  dfree(ctx, b.dofs); dfree(ctx, b.vals); dfree(ctx, b.ramp); dfree(ctx, b.fn); dfree(ctx, b.rows);
+  dfree(ctx, b.rptr); dfree(ctx, b.rpos); dfree(ctx, b.rcol); dfree(ctx, b.zpos); dfree(ctx, b.zone);
   b = BcDev();
   b.nbc = (int)dofs.size();
   b.nrows = (int)rows.size();
@@ -1620,6 +1689,7 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   CK(upload(ctx, &b.rcol, rcol));
   CK(upload(ctx, &b.zpos, zpos));
   CK(upload(ctx, &b.zone, zone));
+  ctx->bc_dofs = dofs;
   ctx->bcs_set = true;
   return PFEM_OK;
 }

@@ -473,137 +473,6 @@ void dense_mv(int n, const T* M, const T* b, T* y, cudaStream_t st) {
   pfem::count_launch(); dense_mv_kernel<T><<<blocks, 256, 0, st>>>(n, M, b, y);
 }
 
-// ------------------------------------------------------------------ coarse inverse
-// Dense copy of the coarsest operator (6 x 6 blocks) into a (n x n, FP64, zeroed).
-template <typename T>
-__global__ void coarse_densify_kernel(int nbrow, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                      const T* __restrict__ val, int n, double* __restrict__ a) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nnzb = rowptr[nbrow];
-  if (i >= nnzb * 36) return;
-  const long long k = i / 36;
-  const int rc = (int)(i - k * 36), r = rc / 6, c = rc % 6;
-  int lo = 0, hi = nbrow;  // block row of k: last I with rowptr[I] <= k
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (rowptr[mid] <= k) lo = mid;
-    else hi = mid;
-  }
-  a[(long long)(lo * 6 + r) * n + col[k] * 6 + c] = (double)val[i];
-}
-
-// Gauss-Jordan inverse with partial pivoting of the dense n x n matrix a
-// (FP64, overwritten) by one thread block; inv is FP64 scratch, out receives
-// the inverse in T.  Rows that are entirely zero (rigid modes absent from an
-// aggregate) get a unit diagonal; pivots below 1e-14 max|diag| are replaced
-// by that magnitude.  fcol (dynamic shared memory) holds n doubles.
-template <typename T>
-__global__ void __launch_bounds__(1024) gj_inverse_kernel(int n, double* __restrict__ a, double* __restrict__ inv,
-                                                          T* __restrict__ out) {
-  extern __shared__ double fcol[];
-  __shared__ double red_v[32];
-  __shared__ int red_i[32];
-  __shared__ int s_piv;
-  __shared__ double s_scl;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  const long long nn = (long long)n * n;
-  for (long long i = tid; i < nn; i += nt) inv[i] = (i / n == i % n) ? 1.0 : 0.0;
-  for (int row = warp; row < n; row += nw) {
-    bool nz = false;
-    for (int j = lane; j < n; j += 32) nz |= a[(long long)row * n + j] != 0.0;
-    nz = __any_sync(0xffffffffu, nz);
-    if (!nz && lane == 0) a[(long long)row * n + row] = 1.0;
-  }
-  __syncthreads();
-  // scl = max |a_ii|
-  {
-    double m = 0.0;
-    for (int i = tid; i < n; i += nt) m = fmax(m, fabs(a[(long long)i * n + i]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) red_v[warp] = m;
-    __syncthreads();
-    if (tid == 0) {
-      double s = 0.0;
-      for (int w = 0; w < nw; ++w) s = fmax(s, red_v[w]);
-      s_scl = fmax(s, 1e-300);
-    }
-    __syncthreads();
-  }
-  const double tiny = 1e-14 * s_scl;
-  for (int c = 0; c < n; ++c) {
-    // pivot: first row r >= c of the largest |a[r][c]|
-    double bv = -1.0;
-    int bi = c;
-    for (int r = c + tid; r < n; r += nt) {
-      const double v = fabs(a[(long long)r * n + c]);
-      if (v > bv) { bv = v; bi = r; }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-    }
-    if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
-    __syncthreads();
-    if (tid == 0) {
-      double v = red_v[0];
-      int ix = red_i[0];
-      for (int w = 1; w < nw; ++w)
-        if (red_v[w] > v || (red_v[w] == v && red_i[w] < ix)) { v = red_v[w]; ix = red_i[w]; }
-      s_piv = ix;
-    }
-    __syncthreads();
-    const int piv = s_piv;
-    if (piv != c)
-      for (int j = tid; j < n; j += nt) {
-        const double t1 = a[(long long)c * n + j];
-        a[(long long)c * n + j] = a[(long long)piv * n + j];
-        a[(long long)piv * n + j] = t1;
-        const double t2 = inv[(long long)c * n + j];
-        inv[(long long)c * n + j] = inv[(long long)piv * n + j];
-        inv[(long long)piv * n + j] = t2;
-      }
-    __syncthreads();
-    double pv = a[(long long)c * n + c];
-    if (fabs(pv) < tiny) pv = (pv >= 0.0 ? 1.0 : -1.0) * tiny;
-    const double ip = 1.0 / pv;
-    __syncthreads();  // every thread has read the pivot before row c changes
-    for (int j = tid; j < n; j += nt) {
-      a[(long long)c * n + j] *= ip;
-      inv[(long long)c * n + j] *= ip;
-    }
-    __syncthreads();
-    for (int r = tid; r < n; r += nt) fcol[r] = a[(long long)r * n + c];
-    __syncthreads();
-    for (long long i = tid; i < nn; i += nt) {
-      const int r = (int)(i / n);
-      if (r == c) continue;
-      const double f = fcol[r];
-      if (f == 0.0) continue;
-      const int j = (int)(i - (long long)r * n);
-      a[i] -= f * a[(long long)c * n + j];
-      inv[i] -= f * inv[(long long)c * n + j];
-    }
-    __syncthreads();
-  }
-  for (long long i = tid; i < nn; i += nt) out[i] = (T)inv[i];
-}
-
-template <typename T>
-void coarse_inverse(int nbrow, const int* rowptr, const int* col, long long nnzb, const T* val, int n,
-                    double* work, T* out, cudaStream_t st) {
-  double* a = work;
-  double* inv = work + (long long)n * n;
-  cudaMemsetAsync(a, 0, (size_t)n * n * sizeof(double), st);
-  const long long tot = nnzb * 36;
-  pfem::count_launch();
-  coarse_densify_kernel<T><<<(int)((tot + 255) / 256), 256, 0, st>>>(nbrow, rowptr, col, val, n, a);
-  pfem::count_launch();
-  gj_inverse_kernel<T><<<1, 1024, (size_t)n * sizeof(double), st>>>(n, a, inv, out);
-}
-
 // ------------------------------------------------------------------ smoothed aggregation
 // P = (I - w D^-1 A) T with the tentative T (one bs x 6 block per fine row).
 // One thread per P block p (row n, aggregate J):
@@ -854,9 +723,7 @@ void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
   template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);                            \
   template void sa_setup_level<T>(const AmgLevel<T>&, T, T*, int, cudaStream_t);                   \
   template void sa_restrict<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);                    \
-  template void sa_prolong<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);                     \
-  template void coarse_inverse<T>(int, const int*, const int*, long long, const T*, int, double*, T*,  \
-                                  cudaStream_t);
+  template void sa_prolong<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);
 PFEM_INST(float)
 PFEM_INST(double)
 template void convert<double, float>(long long, const double*, float*, double, cudaStream_t);

@@ -51,9 +51,5 @@ template <typename T> void dense_mv(int n, const T* M, const T* b, T* y, cudaStr
 template <typename T> void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t st);
 template <typename T> void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st);
 template <typename T> void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st);
-// Inverse of the coarsest operator (6 x 6 block pattern rowptr/col, nnzb blocks)
-// on the device: densify into work (2 n^2 doubles), Gauss-Jordan in FP64, write out (T).
-template <typename T> void coarse_inverse(int nbrow, const int* rowptr, const int* col, long long nnzb,
-                                          const T* val, int n, double* work, T* out, cudaStream_t st);
 
 }  // namespace pfem

@@ -78,8 +78,6 @@ struct Amg {
   VT* coarse_val = nullptr;  // Galerkin operator of the coarsest level (6 x 6 blocks)
   VT* coarse_inv = nullptr;  // coarse_n x coarse_n dense inverse (row-major)
   VT *cx = nullptr, *cb = nullptr;
-  int *c_rowptr = nullptr, *c_col = nullptr;  // coarsest level's 6x6 block pattern (device)
-  double* cwork = nullptr;                     // 2 n^2 doubles: dense coarse operator and its inverse
   bool built = false;
   int cheb_degree = 2;
   long long version = 0;     // bumped by every numeric set-up (captured solver graphs key on it)
