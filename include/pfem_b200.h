@@ -80,6 +80,10 @@ typedef struct pfem_solve_opts {
   int32_t predictor_smooth; /* learned predictor only: degree of the block-Jacobi Chebyshev
                             smoothing applied to the network's correction, on the tangent
                             at the extrapolated guess (0 = none) */
+  int32_t max_cuts;      /* pfem_solve only: a load step that does not converge (or inverts an
+                            element) is retried from the last converged state with half the
+                            increment, at most max_cuts times per load step; 0 = the
+                            reference (solve! stops, Solver.jl:455-466) */
 } pfem_solve_opts;
 
 typedef struct pfem_solve_result {
@@ -93,6 +97,7 @@ typedef struct pfem_solve_result {
   double time_amg_setup_ms;
   double time_krylov_ms;
   double time_predictor_ms;
+  int32_t load_step_cuts;       /* increments halved under pfem_solve_opts.max_cuts */
 } pfem_solve_result;
 
 void pfem_default_opts(pfem_solve_opts* o);

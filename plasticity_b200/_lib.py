@@ -42,7 +42,7 @@ class SolveOpts(C.Structure):
                 ("eta_min", C.c_double), ("eta_max", C.c_double), ("ew_gamma", C.c_double),
                 ("ew_alpha", C.c_double), ("krylov_itmax", C.c_int32), ("predictor", C.c_int32),
                 ("amg_rebuild", C.c_int32), ("cheb_degree", C.c_int32), ("verbose", C.c_int32),
-                ("line_search", C.c_int32), ("predictor_smooth", C.c_int32)]
+                ("line_search", C.c_int32), ("predictor_smooth", C.c_int32), ("max_cuts", C.c_int32)]
 
 
 class SolveResultC(C.Structure):
@@ -50,7 +50,8 @@ class SolveResultC(C.Structure):
                 ("newton_iters_total", C.c_int32), ("krylov_iters_total", C.c_int32),
                 ("predictor_learned_used", C.c_int32), ("time_total_ms", C.c_double),
                 ("time_assembly_ms", C.c_double), ("time_amg_setup_ms", C.c_double),
-                ("time_krylov_ms", C.c_double), ("time_predictor_ms", C.c_double)]
+                ("time_krylov_ms", C.c_double), ("time_predictor_ms", C.c_double),
+                ("load_step_cuts", C.c_int32)]
 
 
 _d = C.POINTER(C.c_double)

@@ -1352,6 +1352,7 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->verbose = 0;
   o->line_search = 0;
   o->predictor_smooth = 16;
+  o->max_cuts = 0;
 }
 
 const char* pfem_last_error(const pfem_ctx* ctx) {
@@ -1966,29 +1967,45 @@ int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res, 
   int rc = pfem_reset(ctx);
   if (rc) return rc;
   StepTimes tm;
-  for (int n = 1; n <= o->nsteps; ++n) {
-    const double lam = (double)n / o->nsteps;
-    if (o->verbose) fprintf(stderr, "Load step %d/%d  (lambda=%g)\n", n, o->nsteps, lam);
-    bool hf = false;
-    double r0 = 0;
-    rc = step_begin(ctx, lam, o, &tm, &hf, &r0);
-    if (rc) return rc;
-    bool conv = false;
-    int it = 0;
-    rc = newton_dev(ctx, lam, o, &it, residuals ? residuals + (size_t)(n - 1) * o->maxiter : nullptr,
-                    krylov_per_iter ? krylov_per_iter + (size_t)(n - 1) * o->maxiter : nullptr, &conv, &tm, hf, r0);
-    if (rc) return rc;
-    if (iters_per_step) iters_per_step[n - 1] = it;
-    r.newton_iters_total += it;
-    if (!conv) {
-      r.converged = 0;
-      break;
+  for (int n = 1; n <= o->nsteps && r.converged; ++n) {
+    const double lam_n = (double)n / o->nsteps;
+    double lam = lam_n;
+    int cuts = 0;
+    for (;;) {
+      if (o->verbose) fprintf(stderr, "Load step %d/%d  (lambda=%g)\n", n, o->nsteps, lam);
+      bool hf = false, conv = false;
+      double r0 = 0;
+      int it = 0;
+      rc = step_begin(ctx, lam, o, &tm, &hf, &r0);
+      if (rc == PFEM_OK)
+        rc = newton_dev(ctx, lam, o, &it, residuals ? residuals + (size_t)(n - 1) * o->maxiter : nullptr,
+                        krylov_per_iter ? krylov_per_iter + (size_t)(n - 1) * o->maxiter : nullptr, &conv, &tm, hf,
+                        r0);
+      r.newton_iters_total += it;
+      if (iters_per_step) iters_per_step[n - 1] = it;  // the last attempt, matching its residual history
+      const bool soft = rc == PFEM_ERR_NOT_CONVERGED || rc == PFEM_ERR_INVERTED_ELEMENT;
+      if (rc && !soft) return rc;
+      if (rc == PFEM_OK && conv) {
+        rc = commit_dev(ctx);
+        if (rc) return rc;
+        rc = step_end(ctx, lam);
+        if (rc) return rc;
+        if (lam >= lam_n) break;
+        lam = lam_n;  // a cut sub-step converged: go on to the load step's own load factor
+        continue;
+      }
+      if (cuts >= o->max_cuts) {
+        r.converged = 0;
+        break;
+      }
+      // retry from the last converged state with half the increment
+      ++cuts;
+      ++r.load_step_cuts;
+      CK(cudaMemcpyAsync(ctx->dU, ctx->dUprev, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
+      lam = ctx->lam_prev + 0.5 * (lam - ctx->lam_prev);
+      ctx->err.clear();
     }
-    rc = commit_dev(ctx);
-    if (rc) return rc;
-    rc = step_end(ctx, lam);
-    if (rc) return rc;
-    r.steps_done = n;
+    if (r.converged) r.steps_done = n;
   }
   CK(cudaStreamSynchronize(ctx->st));
   r.krylov_iters_total = tm.kits;

@@ -259,7 +259,7 @@ class Model:
 
     def _opts(self, nsteps=10, tol=1e-8, maxiter=25, precision="fp64", linsolve="cg", lin_rtol=None,
               predictor="previous", amg_rebuild=False, cheb_degree=2, cg_itmax=200, eta_min=None,
-              line_search=False, verbose=False, predictor_smooth=None, eta_max=None):
+              line_search=False, verbose=False, predictor_smooth=None, eta_max=None, max_cuts=0):
         o = L.SolveOpts()
         L.lib().pfem_default_opts(C.byref(o))
         o.nsteps, o.maxiter, o.tol = nsteps, maxiter, tol
@@ -280,6 +280,7 @@ class Model:
             o.predictor_smooth = int(predictor_smooth)
         if eta_max is not None:
             o.eta_max = float(eta_max)
+        o.max_cuts = int(max_cuts)
         return o
 
     def solve(self, nsteps=10, tol=1e-8, maxiter=25, **kw) -> SolveResult:

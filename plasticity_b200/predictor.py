@@ -53,11 +53,13 @@ def run_path(M, w, predictor, precision="mixed", tol=1e-8):
     w.apply(M)
     t0 = time.perf_counter()
     r = M.solve(nsteps=w.nsteps, tol=tol, maxiter=60, precision=precision, predictor=predictor,
-                line_search=True)
+                line_search=True, max_cuts=4)
     sec = time.perf_counter() - t0
     return dict(converged=r.converged, newton=list(r.iters), krylov=[int(sum(k)) for k in r.cg_iters],
                 first_residual=[float(h[0]) for h in r.residuals], seconds=sec,
-                learned_used=int(r.stats["predictor_learned_used"]), stats=r.stats)
+                learned_used=int(r.stats["predictor_learned_used"]), cuts=int(r.stats["load_step_cuts"]),
+                newton_total=int(r.stats["newton_iters_total"]), krylov_total=int(r.stats["krylov_iters_total"]),
+                stats=r.stats)
 
 
 def guess_errors(M, w, smooth=None, precision="mixed", tol=1e-10):
@@ -166,8 +168,10 @@ def main():
                 load_into(M, args.out)
             rows = [run_path(M, W.config4_path(n=args.n, seed=args.seed0 + i), pred) for i in range(args.paths)]
             out[pred] = dict(converged=all(r["converged"] for r in rows),
-                             newton=int(sum(sum(r["newton"]) for r in rows)),
-                             krylov=int(sum(sum(r["krylov"]) for r in rows)),
+                             paths_converged=int(sum(r["converged"] for r in rows)),
+                             load_step_cuts=int(sum(r["cuts"] for r in rows)),
+                             newton=int(sum(r["newton_total"] for r in rows)),
+                             krylov=int(sum(r["krylov_total"] for r in rows)),
                              seconds=float(sum(r["seconds"] for r in rows)),
                              learned_used=int(sum(r["learned_used"] for r in rows)),
                              steps=int(sum(len(r["newton"]) for r in rows)))

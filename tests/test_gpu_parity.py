@@ -208,3 +208,16 @@ def test_reused_model_takes_new_boundary_values():
     wb.apply(F)
     F.solve(nsteps=4, tol=1e-10, maxiter=40, line_search=True)
     assert rel(M.U, F.U) < 1e-12
+
+
+def test_load_step_cutting_recovers_a_failed_increment():
+    """10 % compression per increment fails (the reference stops); with max_cuts the
+    failed increments are retried at half size and the path completes."""
+    w = W.config2(n=4, nsteps=2)
+    M = model_from(w)
+    plain = M.solve(nsteps=2, tol=1e-8, maxiter=25, line_search=True)
+    assert not plain.converged
+    M = model_from(w)
+    cut = M.solve(nsteps=2, tol=1e-8, maxiter=25, line_search=True, max_cuts=8)
+    assert cut.converged and cut.stats["load_step_cuts"] > 0, cut.stats
+    assert len(cut.iters) == 2
