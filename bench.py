@@ -313,6 +313,24 @@ def main():
                                            "plain_fp64": float(np.linalg.norm(U_fp64 - U_true) / nrm),
                                            "fp64_extrapolate": float(np.linalg.norm(U_fx - U_true) / nrm)}}
 
+    # ---- the whole load path through pfem_solve (solve!): nsteps / wall time, model built ----
+    full = {}
+    if not args.no_compare:
+        for name, kind in (("mixed_learned", "mixed"), ("plain_fp64", "fp64")):
+            Mf = fresh_model()
+            barrier()
+            r = Mf.solve(nsteps=w.nsteps, tol=w.tol, maxiter=60, max_cuts=4, **solver_kw(kind, have_mlp))
+            st = r.stats
+            full[name] = {"converged": bool(r.converged), "load_steps_per_s": w.nsteps / (st["time_total_ms"] / 1e3),
+                          "wall_s": st["time_total_ms"] / 1e3, "newton_total": int(st["newton_iters_total"]),
+                          "krylov_total": int(st["krylov_iters_total"]),
+                          "amg_setup_s": st["time_amg_setup_ms"] / 1e3, "load_step_cuts": int(st["load_step_cuts"])}
+            del Mf
+        full["speedup"] = full["mixed_learned"]["load_steps_per_s"] / full["plain_fp64"]["load_steps_per_s"]
+        full["what"] = (f"all {w.nsteps} increments through pfem_solve (solve!): load steps / its wall time, "
+                        "model construction excluded, AMG set-up included and reported")
+        out_extra["full_path"] = full
+
     # ---- e2e: the same increments through the public C-ABI calls from host buffers ----
     t_build = time.perf_counter()
     Me = P.Model(w.mesh, mat, sigy0_e=w.sigy0_e, device=local)
