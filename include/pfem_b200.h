@@ -42,7 +42,10 @@ enum pfem_status {
 };
 
 /* Element kinds, FiniteStrain.jl:62-65 (Hex8Finite / Hex8FiniteFbar). */
-enum pfem_kind { PFEM_HEX8_FINITE = 1, PFEM_HEX8_FINITE_FBAR = 2 };
+/* Element kinds (Model(...; element=:small / :finite / :finite_fbar), Model.jl:63-75).
+ * PFEM_HEX8_SMALL: small strain (Elements.jl:323-360); the committed plastic strain lives in
+ * the eps_p state array and the stress outputs are sigma. */
+enum pfem_kind { PFEM_HEX8_SMALL = 0, PFEM_HEX8_FINITE = 1, PFEM_HEX8_FINITE_FBAR = 2 };
 /* Tangent / inner-solve precision: FP64 throughout, or FP32 tangent + FP32
  * Krylov/AMG inside the FP64 Newton residual loop. */
 enum pfem_precision { PFEM_FP64 = 0, PFEM_MIXED = 1 };

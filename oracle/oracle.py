@@ -139,11 +139,13 @@ def finite_update(mat, F, cpi=None, alpha=0.0):
 
 
 def element(fbar, mat, Xe, ue, cpi=None, alpha=None, sigy0=None):
-    """One Hex8 element (Elements.jl:405-494).  Xe (8,3), ue (24,).  Returns dict."""
+    """One Hex8 element: fbar 0 / 1 finite strain without / with F-bar
+    (Elements.jl:405-494), 2 small strain (Elements.jl:323-360; cpi is then eps_p,
+    tau is sigma).  Xe (8,3), ue (24,).  Returns dict."""
     Xe = np.ascontiguousarray(np.asarray(Xe, np.float64).reshape(24))
     ue = np.ascontiguousarray(np.asarray(ue, np.float64).reshape(24))
     if cpi is None:
-        cpi = np.tile([1, 1, 1, 0, 0, 0.0], 8)
+        cpi = np.zeros(48) if int(fbar) == 2 else np.tile([1, 1, 1, 0, 0, 0.0], 8)
     cpi = np.ascontiguousarray(np.asarray(cpi, np.float64).reshape(48))
     alpha = np.zeros(8) if alpha is None else np.ascontiguousarray(alpha, np.float64)
     Fe, Ke, tau, cn, an, ei = (np.zeros(24), np.zeros(576), np.zeros(48), np.zeros(48),
@@ -209,11 +211,12 @@ def element_colors(nodes, elems):
 # ---------------------------------------------------------------- model
 @dataclass
 class OracleModel:
-    """Model (Model.jl:32-75) restated for the F-bar / finite kinds."""
+    """Model (Model.jl:32-75) restated for the F-bar / finite / small-strain kinds."""
     nodes: np.ndarray            # (3, nn)
     elems: np.ndarray            # (8, ne) 1-based
     mat: J2Material
     fbar: bool = True
+    small: bool = False          # small-strain kind (Elements.jl:323-360); fbar is then ignored
     sigy0_e: np.ndarray | None = None
     nthreads: int = 0
     dir_dofs: list = field(default_factory=list)
@@ -262,7 +265,9 @@ class OracleModel:
     def reset(self):
         ngp = 8 * self.ne
         self.U = np.zeros(self.ndof)
-        self.cpi = np.zeros((ngp, 6)); self.cpi[:, :3] = 1.0
+        self.cpi = np.zeros((ngp, 6))    # Cp^-1 (finite kinds) or eps_p (small strain)
+        if not self.small:
+            self.cpi[:, :3] = 1.0
         self.alpha = np.zeros(ngp)
         self.epsp = np.zeros((ngp, 6))
         self.tau = np.zeros((ngp, 6))
@@ -280,7 +285,7 @@ class OracleModel:
         be = C.c_int64(0); bg = C.c_int(0); bJ = C.c_double(0)
         U = np.ascontiguousarray(U, np.float64)
         m5 = _mat5(self.mat)
-        st = lib().or_assemble(int(self.fbar), _p(m5), _p(self.sigy0_e), self.nn, self.ne,
+        st = lib().or_assemble(2 if self.small else int(self.fbar), _p(m5), _p(self.sigy0_e), self.nn, self.ne,
                                _p(self._nodes_rm), _p(self._el_rm, _i64), _p(self.colptr, _i64),
                                _p(self.rowval, _i64), _p(U), _p(cpi), _p(alpha),
                                _p(self.epsp), int(commit), _p(nz), _p(R), _p(tau),
@@ -387,7 +392,10 @@ class OracleModel:
         return self.U.reshape(-1, 3).T.copy()
 
     def gauss_stress(self):
-        """Cauchy = tau / det F_gp (standard F, not F-bar), Model.jl:188-208."""
+        """Cauchy = tau / det F_gp (standard F, not F-bar), Model.jl:188-208; the
+        small-strain kind stores sigma itself."""
+        if self.small:
+            return self.tau.copy()
         from_gp = np.zeros_like(self.tau)
         detF = gp_detF(self.nodes, self.elems, self.U)
         invJ = np.where(detF > 0, 1.0 / np.where(detF > 0, detF, 1.0), 1.0)

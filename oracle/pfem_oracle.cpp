@@ -464,8 +464,10 @@ int or_finite_update(const double* mat5, const double* F9, const double* cpi6, d
 }
 
 // Element force / tangent for one Hex8 element,
-// element_force_tangent_finite!, Elements.jl:405-494 (Hkin = 0), with the
-// F-bar chain of _fbar_Geff, Elements.jl:524-531.
+// fbar = 0: element_force_tangent_finite!, Elements.jl:405-494 (Hkin = 0);
+// fbar = 1: the same with the
+// F-bar chain of _fbar_Geff, Elements.jl:524-531; fbar = 2: the small-strain
+// element_force_tangent!, Elements.jl:323-360 (state slot = eps_p, tau = sigma).
 //   Xe24: node-major coordinates (a*3 + d); ue24 node-major displacements.
 //   cpi48 / alpha8: committed state per Gauss point (g*6 + c, g).
 //   Ke576 row-major 24x24.  tau48 Kirchhoff stress per GP.  flags8 = f_tr>0.
@@ -478,6 +480,66 @@ int or_element(int fbar, const double* mat5, double sigy0, const double* Xe24,
   double Xe[8][3];
   for (int a = 0; a < 8; ++a)
     for (int d = 0; d < 3; ++d) Xe[a][d] = Xe24[a * 3 + d];
+  if (fbar == 2) {
+    // Small strain: element_force_tangent!, Elements.jl:323-360, with bmatrix
+    // :97-117 and return_map (Hkin = 0, so beta stays zero).  The state slot
+    // cpi48 carries eps_p (6 per GP, engineering shear), tau48 receives sigma.
+    const double g = 1.0 / std::sqrt(3.0);
+    std::memset(Fe24, 0, 24 * sizeof(double));
+    std::memset(Ke576, 0, 576 * sizeof(double));
+    const double beta0[6] = {0, 0, 0, 0, 0, 0};
+    for (int gp = 0; gp < 8; ++gp) {
+      const double xi[3] = {GSGN[gp][0] * g, GSGN[gp][1] * g, GSGN[gp][2] * g};
+      double dNdX[8][3];
+      const double w = ref_grads(Xe, xi, dNdX);
+      double B[6 * 24];
+      std::memset(B, 0, sizeof(B));
+      for (int a = 0; a < 8; ++a) {
+        const double Nx = dNdX[a][0], Ny = dNdX[a][1], Nz = dNdX[a][2];
+        B[0 * 24 + 3 * a + 0] = Nx;
+        B[1 * 24 + 3 * a + 1] = Ny;
+        B[2 * 24 + 3 * a + 2] = Nz;
+        B[3 * 24 + 3 * a + 0] = Ny; B[3 * 24 + 3 * a + 1] = Nx;
+        B[4 * 24 + 3 * a + 1] = Nz; B[4 * 24 + 3 * a + 2] = Ny;
+        B[5 * 24 + 3 * a + 0] = Nz; B[5 * 24 + 3 * a + 2] = Nx;
+      }
+      double eps[6];
+      for (int r = 0; r < 6; ++r) {
+        double t = 0.0;
+        for (int c = 0; c < 24; ++c) t += B[r * 24 + c] * ue24[c];
+        eps[r] = t;
+      }
+      double sig[6], ep_new[6], b_new[6], a_new, D[36];
+      const int pl = return_map(m, sigy0, eps, cpi48 + gp * 6, beta0, alpha8[gp], sig, ep_new, b_new, &a_new,
+                                D, nullptr);
+      for (int c = 0; c < 24; ++c) {
+        double t = 0.0;
+        for (int r = 0; r < 6; ++r) t += B[r * 24 + c] * sig[r];
+        Fe24[c] += t * w;
+      }
+      double DB[6 * 24];
+      for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 24; ++c) {
+          double t = 0.0;
+          for (int q = 0; q < 6; ++q) t += D[r * 6 + q] * B[q * 24 + c];
+          DB[r * 24 + c] = t;
+        }
+      for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) {
+          double t = 0.0;
+          for (int r = 0; r < 6; ++r) t += B[r * 24 + i] * DB[r * 24 + j];
+          Ke576[i * 24 + j] += t * w;
+        }
+      for (int c = 0; c < 6; ++c) {
+        if (tau48) tau48[gp * 6 + c] = sig[c];
+        if (cpi_new48) cpi_new48[gp * 6 + c] = ep_new[c];
+        if (epsp_inc48) epsp_inc48[gp * 6 + c] = ep_new[c] - cpi48[gp * 6 + c];
+      }
+      if (alpha_new8) alpha_new8[gp] = a_new;
+      if (flags8) flags8[gp] = (unsigned char)pl;
+    }
+    return 0;
+  }
   const double g = 1.0 / std::sqrt(3.0);
   double dNdX0[8][3], F0[3][3], J0 = 1.0, g0[24];
   if (fbar) {

@@ -20,6 +20,7 @@ PFEM_ERR_LINSOLVE = -4
 PFEM_ERR_NOT_CONVERGED = -5
 PFEM_ERR_STATE = -6
 
+PFEM_HEX8_SMALL = 0
 PFEM_HEX8_FINITE = 1
 PFEM_HEX8_FINITE_FBAR = 2
 PFEM_FP64 = 0

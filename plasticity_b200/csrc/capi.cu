@@ -1028,6 +1028,7 @@ int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* 
 int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
   cudaStream_t st = ctx->st;
   const bool fbar = ctx->kind == PFEM_HEX8_FINITE_FBAR;
+  const bool small = ctx->kind == PFEM_HEX8_SMALL;
   CK(cudaMemsetAsync(ctx->dStatus, 0, sizeof(DevStatus), st));
   if (commit) {
     ElemArgs<double> a{};
@@ -1035,7 +1036,8 @@ int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
     a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
     a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
-    launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, true, fbar, st);
+    if (small) launch_element_small<double>(a, ctx->dAllElems, (int)ctx->ne, true, st);
+    else launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, true, fbar, st);
     CKL();
     return PFEM_OK;
   }
@@ -1048,9 +1050,12 @@ int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
     a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
     a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
-    for (int c = 0; c < nc; ++c)
-      launch_element_color<double>(a, ctx->dColorList + ctx->color_ptr[c], ctx->color_ptr[c + 1] - ctx->color_ptr[c],
-                                   false, fbar, st);
+    for (int c = 0; c < nc; ++c) {
+      const int* cl = ctx->dColorList + ctx->color_ptr[c];
+      const int cn = ctx->color_ptr[c + 1] - ctx->color_ptr[c];
+      if (small) launch_element_small<double>(a, cl, cn, false, st);
+      else launch_element_color<double>(a, cl, cn, false, fbar, st);
+    }
   } else {
     CK(cudaMemsetAsync(ctx->dK32, 0, (size_t)ctx->nnzb * 9 * sizeof(float), st));
     ElemArgs<float> a{};
@@ -1058,9 +1063,12 @@ int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
     a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
     a.R = ctx->dR; a.Kval = ctx->dK32; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
-    for (int c = 0; c < nc; ++c)
-      launch_element_color<float>(a, ctx->dColorList + ctx->color_ptr[c], ctx->color_ptr[c + 1] - ctx->color_ptr[c],
-                                  false, fbar, st);
+    for (int c = 0; c < nc; ++c) {
+      const int* cl = ctx->dColorList + ctx->color_ptr[c];
+      const int cn = ctx->color_ptr[c + 1] - ctx->color_ptr[c];
+      if (small) launch_element_small<float>(a, cl, cn, false, st);
+      else launch_element_color<float>(a, cl, cn, false, fbar, st);
+    }
   }
   CKL();
   return PFEM_OK;
@@ -1373,8 +1381,8 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     g_cuda_err = "this path implements linear isotropic hardening only (Hkin must be 0)";
     return PFEM_ERR_BAD_ARG;
   }
-  if (kind != PFEM_HEX8_FINITE && kind != PFEM_HEX8_FINITE_FBAR) {
-    g_cuda_err = "kind must be PFEM_HEX8_FINITE or PFEM_HEX8_FINITE_FBAR";
+  if (kind != PFEM_HEX8_SMALL && kind != PFEM_HEX8_FINITE && kind != PFEM_HEX8_FINITE_FBAR) {
+    g_cuda_err = "kind must be PFEM_HEX8_SMALL, PFEM_HEX8_FINITE or PFEM_HEX8_FINITE_FBAR";
     return PFEM_ERR_BAD_ARG;
   }
   for (int64_t i = 0; i < 8 * ne; ++i)
@@ -2123,6 +2131,8 @@ int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, d
 
 int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma) {
   if (!ctx || !sigma) return PFEM_ERR_BAD_ARG;
+  // the small-strain kind stores sigma itself (Model.jl:188-208, small branch)
+  if (ctx->kind == PFEM_HEX8_SMALL) return pfem_get_state(ctx, nullptr, sigma, nullptr, nullptr, nullptr, nullptr);
   // tau / det F at each Gauss point with the standard F (Model.jl:188-208)
   std::vector<double> U(ctx->ndof);
   int rc = pfem_get_state(ctx, U.data(), sigma, nullptr, nullptr, nullptr, nullptr);

@@ -488,6 +488,250 @@ static void launch_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_
   pfem::count_launch(); element_color_kernel<KT, COMMIT, FBAR><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
 }
 
+// ---------------------------------------------------------------- small strain
+// The small-strain kind, element_force_tangent! (Elements.jl:323-360) with
+// bmatrix (:97-117) and the Voigt return map (Materials.jl:159-250, linear
+// isotropic hardening, Hkin = 0 so the back stress stays zero).  Same warp
+// organisation as the finite kernel: a lane evaluates one Gauss point
+// (strain, return map, stress, consistent tangent D in FP64), the forces are
+// shuffle-reduced node by node, the records (dN/dX, w D) go to shared memory in
+// the tangent's type and the warp's 4 x 24 K_e columns are summed over the
+// eight Gauss points by all 32 lanes and added into the tangent.  The state
+// array epsp holds the committed plastic strain, tau receives sigma.
+constexpr int SREC = 24 + 36;                 // dN/dX, w D (row-major 6 x 6)
+constexpr int SSLOT = 8 * SREC;
+template <typename TT>
+constexpr int warp_smem_small(bool commit) {
+  return commit ? EPW * 48 * 8 : EPW * SSLOT * (int)sizeof(TT);
+}
+static_assert(8 * SREC * 4 >= 48 * 8, "coordinate scratch must fit in the record area");
+
+template <typename KT, bool COMMIT>
+__global__ void __launch_bounds__(32 * WPB)
+element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
+  using TT = KT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = lane >> 3, g = lane & 7;
+  const long long li = ((long long)blockIdx.x * WPB + warp) * EPW + slot;
+  const bool valid = li < nlist;
+  const int e = elist[valid ? li : 0];
+  TT* const wbase = reinterpret_cast<TT*>(smem_raw) + warp * EPW * SSLOT;
+  TT* const S = wbase + slot * SSLOT;
+  TT* const Rg = S + g * SREC;
+  double* const XU = COMMIT ? reinterpret_cast<double*>(smem_raw) + (warp * EPW + slot) * 48
+                            : reinterpret_cast<double*>(S);
+  double* const Xe = XU;
+  double* const ue = XU + 24;
+  __shared__ int nodes_s[WPB][EPW][8];
+  {
+    const int nd = p.elem[(long long)e * 8 + g];
+    nodes_s[warp][slot][g] = nd;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      Xe[g * 3 + d] = p.X[(long long)nd * 3 + d];
+      ue[g * 3 + d] = p.U[(long long)nd * 3 + d];
+    }
+  }
+  __syncwarp();
+  const MatParams m = p.mat;
+  const long long gp = (long long)e * 8 + g;
+  const double gc = 0.57735026918962576451;
+  const double xg = nsgn_x(g) * gc, yg = nsgn_y(g) * gc, zg = nsgn_z(g) * gc;
+  double Jm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double d[3];
+    dshape_a(a, xg, yg, zg, d);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Jm[3 * i + j] += Xe[a * 3 + i] * d[j];
+  }
+  const double w = det3(Jm);
+  double Ji[9];
+  inv3(Jm, Ji);
+  // strain eps = B u (engineering shear), bmatrix Elements.jl:97-117
+  double eps[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double d[3];
+    dshape_a(a, xg, yg, zg, d);
+    const double nx = d[0] * Ji[0] + d[1] * Ji[3] + d[2] * Ji[6];
+    const double ny = d[0] * Ji[1] + d[1] * Ji[4] + d[2] * Ji[7];
+    const double nz = d[0] * Ji[2] + d[1] * Ji[5] + d[2] * Ji[8];
+    const double ux = ue[a * 3], uy = ue[a * 3 + 1], uz = ue[a * 3 + 2];
+    eps[0] += nx * ux;
+    eps[1] += ny * uy;
+    eps[2] += nz * uz;
+    eps[3] += ny * ux + nx * uy;
+    eps[4] += nz * uy + ny * uz;
+    eps[5] += nz * ux + nx * uz;
+  }
+  __syncwarp();  // the nodal coordinates are dead; the records may overwrite them
+  // ---- return_map, Materials.jl:159-250 (Hkin = 0, beta = 0) ----
+  const double G = m.G, lam = m.lam, H = m.Hiso;
+  const double sy0 = p.sigy0_e ? p.sigy0_e[e] : m.sigy0;
+  const double an = p.alpha[gp];
+  double de[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) de[c] = eps[c] - p.epsp[(long long)c * p.ngp + gp];
+  const double tr = de[0] + de[1] + de[2];
+  double st[6];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) st[c] = lam * tr + 2.0 * G * de[c];
+#pragma unroll
+  for (int c = 3; c < 6; ++c) st[c] = G * de[c];
+  const double pm = (st[0] + st[1] + st[2]) / 3.0;
+  double xi[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) xi[c] = st[c] - (c < 3 ? pm : 0.0);
+  const double nrm = sqrt(xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2] +
+                          2.0 * (xi[3] * xi[3] + xi[4] * xi[4] + xi[5] * xi[5]));
+  const double s32 = 1.22474487139158904910;
+  const double qtr = s32 * nrm;
+  const double ftr = qtr - (sy0 + H * an);
+  const bool plastic = ftr > 0.0;
+  double nh[6] = {0, 0, 0, 0, 0, 0}, sig[6], dg = 0.0, b0 = 0.0, g0c = 0.0;
+  if (plastic) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) nh[c] = xi[c] / nrm;
+    dg = ftr / (3.0 * G + H);
+    b0 = 2.0 * G * dg / qtr;
+    g0c = 2.0 * G / (3.0 * G + H);
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) sig[c] = st[c] - (2.0 * G * dg * s32) * nh[c];
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) p.tau[(long long)c * p.ngp + gp] = sig[c];
+    p.flags[gp] = plastic ? 1 : 0;
+  }
+  if constexpr (COMMIT) {
+    if (!valid) return;
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+      p.epsp[(long long)c * p.ngp + gp] += (dg * s32) * (c < 3 ? nh[c] : 2.0 * nh[c]);
+    p.alpha[gp] = an + dg;
+  } else {
+    // ---- internal force, node by node (FP64), lane g keeps node g ----
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      double d[3];
+      dshape_a(a, xg, yg, zg, d);
+      const double nx = d[0] * Ji[0] + d[1] * Ji[3] + d[2] * Ji[6];
+      const double ny = d[0] * Ji[1] + d[1] * Ji[4] + d[2] * Ji[7];
+      const double nz = d[0] * Ji[2] + d[1] * Ji[5] + d[2] * Ji[8];
+      Rg[a * 3 + 0] = (TT)nx;
+      Rg[a * 3 + 1] = (TT)ny;
+      Rg[a * 3 + 2] = (TT)nz;
+      double v0 = w * (nx * sig[0] + ny * sig[3] + nz * sig[5]);
+      double v1 = w * (ny * sig[1] + nx * sig[3] + nz * sig[4]);
+      double v2 = w * (nz * sig[2] + ny * sig[4] + nx * sig[5]);
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+        v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+      }
+      if (a == g) { f0 = v0; f1 = v1; f2 = v2; }
+    }
+    if (valid) {
+      const int nd = nodes_s[warp][slot][g];
+      p.R[(long long)nd * 3 + 0] += f0;
+      p.R[(long long)nd * 3 + 1] += f1;
+      p.R[(long long)nd * 3 + 2] += f2;
+    }
+    // ---- w D: D = C - 3G b0 Idev + 3G (b0 - g0) n n^T (Materials.jl:245-247) ----
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const double c = (i < 3 && j < 3) ? (i == j ? lam + 2.0 * G : lam) : (i == j ? G : 0.0);
+        const double isym = (i == j) ? (i < 3 ? 1.0 : 0.5) : 0.0;
+        const double idev = isym - ((i < 3 && j < 3) ? 1.0 / 3.0 : 0.0);
+        const double dv = c - (3.0 * G * b0) * idev + (3.0 * G * (b0 - g0c)) * nh[i] * nh[j];
+        Rg[24 + i * 6 + j] = (TT)(w * dv);
+      }
+    __syncwarp();
+    // ---- K_e columns over all 32 lanes, colored scatter ----
+#pragma unroll 1
+    for (int t = lane; t < EPW * 24; t += 32) {
+      const int s2 = t / 24, col = t - 24 * s2;
+      const long long ls = ((long long)blockIdx.x * WPB + warp) * EPW + s2;
+      if (ls >= nlist) continue;
+      const int es = elist[ls];
+      const TT* Ss = wbase + s2 * SSLOT;
+      const int b = col / 3, k = col - 3 * b;
+      TT acc[24];
+#pragma unroll
+      for (int r = 0; r < 24; ++r) acc[r] = TT(0);
+#pragma unroll 1
+      for (int gg = 0; gg < 8; ++gg) {
+        const TT* Rr = Ss + gg * SREC;
+        const TT* dX = Rr;
+        const TT* D = Rr + 24;
+        const TT bx = dX[b * 3], by = dX[b * 3 + 1], bz = dX[b * 3 + 2];
+        TT bc[6];  // column (b,k) of B
+        bc[0] = k == 0 ? bx : TT(0);
+        bc[1] = k == 1 ? by : TT(0);
+        bc[2] = k == 2 ? bz : TT(0);
+        bc[3] = k == 0 ? by : (k == 1 ? bx : TT(0));
+        bc[4] = k == 1 ? bz : (k == 2 ? by : TT(0));
+        bc[5] = k == 0 ? bz : (k == 2 ? bx : TT(0));
+        TT T[6];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          TT v = TT(0);
+#pragma unroll
+          for (int q = 0; q < 6; ++q) v += D[r * 6 + q] * bc[q];
+          T[r] = v;
+        }
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+          const TT x0 = dX[a * 3], x1 = dX[a * 3 + 1], x2 = dX[a * 3 + 2];
+          acc[a * 3 + 0] += x0 * T[0] + x1 * T[3] + x2 * T[5];
+          acc[a * 3 + 1] += x1 * T[1] + x0 * T[3] + x2 * T[4];
+          acc[a * 3 + 2] += x2 * T[2] + x1 * T[4] + x0 * T[5];
+        }
+      }
+      const int* nds = nodes_s[warp][s2];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const long long blk = (long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b];
+        KT* v = p.Kval + blk * 9 + k;
+        v[0] += (KT)acc[a * 3 + 0];
+        v[3] += (KT)acc[a * 3 + 1];
+        v[6] += (KT)acc[a * 3 + 2];
+      }
+    }
+  }
+}
+
+template <typename KT, bool COMMIT>
+static void launch_small_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  const int warps = (n + EPW - 1) / EPW;
+  const int blocks = (warps + WPB - 1) / WPB;
+  const size_t sm = (size_t)WPB * warp_smem_small<KT>(COMMIT);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(element_small_kernel<KT, COMMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = true;
+  }
+  pfem::count_launch();
+  element_small_kernel<KT, COMMIT><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
+}
+
+template <typename KT>
+void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, cudaStream_t st) {
+  if (commit) launch_small_t<KT, true>(a, elist, n, st);
+  else launch_small_t<KT, false>(a, elist, n, st);
+}
+template void launch_element_small<double>(const ElemArgs<double>&, const int*, int, bool, cudaStream_t);
+template void launch_element_small<float>(const ElemArgs<float>&, const int*, int, bool, cudaStream_t);
+
 template <typename KT>
 void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit,
                           bool fbar, cudaStream_t st) {

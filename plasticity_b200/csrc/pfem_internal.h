@@ -32,6 +32,10 @@ struct ElemArgs {
 template <typename KT>
 void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit, bool fbar,
                           cudaStream_t st);
+// Small-strain kind (Elements.jl:323-360): epsp holds the committed plastic
+// strain, tau receives sigma; cpi is unused.
+template <typename KT>
+void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, cudaStream_t st);
 
 // ---------------- block-CSR matrices ----------------
 template <typename VT>

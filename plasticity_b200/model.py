@@ -124,7 +124,7 @@ class SolveResult:
     stats: dict = field(default_factory=dict)
 
 
-_KINDS = {"finite": L.PFEM_HEX8_FINITE, "finite_fbar": L.PFEM_HEX8_FINITE_FBAR}
+_KINDS = {"small": L.PFEM_HEX8_SMALL, "finite": L.PFEM_HEX8_FINITE, "finite_fbar": L.PFEM_HEX8_FINITE_FBAR}
 _PREC = {"fp64": L.PFEM_FP64, "mixed": L.PFEM_MIXED}
 _PRED = {"previous": L.PFEM_PRED_PREVIOUS, "extrapolate": L.PFEM_PRED_EXTRAPOLATE,
          "learned": L.PFEM_PRED_LEARNED}
@@ -141,7 +141,7 @@ class Model:
                  sigy0_e=None, device: int = 0):
         element = element.lstrip(":")
         if element not in _KINDS:
-            raise ValueError(f"unknown element kind {element} (use finite, finite_fbar)")
+            raise ValueError(f"unknown element kind {element} (use small, finite, finite_fbar)")
         self.mesh = mesh
         self.material = material
         self.element = element

@@ -278,3 +278,27 @@ def test_F11_fbar_newton_converges_quadratically(oracle):
     assert m.alpha.max() > 0.05
     h = res["residuals"][-1]
     assert any(h[k + 1] <= 50 * h[k] ** 2 + 1e-12 for k in range(1, len(h) - 1) if h[k] < 1)
+
+
+def test_small_strain_element_fd_tangent_and_symmetry(oracle):
+    """Small-strain kind (Elements.jl:323-360): the consistent tangent K_e matches
+    central differences of F_e on a plastic state and is symmetric (associative J2)."""
+    rng = np.random.default_rng(3)
+    mat = oracle.J2Material(200e3, 0.3, 250.0, 2000.0)
+    nat = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                    [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], float)
+    Xe = 0.5 * (nat + 1) + 0.08 * rng.standard_normal((8, 3))
+    ue = 0.004 * rng.standard_normal(24)
+    epsp = 1e-4 * rng.standard_normal(48)
+    alpha = 1e-4 * rng.random(8)
+    out = oracle.element(2, mat, Xe, ue, cpi=epsp, alpha=alpha)
+    assert out["flags"].sum() >= 4
+    K = out["Ke"]
+    h = 1e-8
+    Kfd = np.zeros((24, 24))
+    for j in range(24):
+        e = np.zeros(24); e[j] = h
+        Kfd[:, j] = (oracle.element(2, mat, Xe, ue + e, cpi=epsp, alpha=alpha)["Fe"]
+                     - oracle.element(2, mat, Xe, ue - e, cpi=epsp, alpha=alpha)["Fe"]) / (2 * h)
+    assert np.abs(K - Kfd).max() <= 1e-6 * np.abs(K).max()
+    assert np.abs(K - K.T).max() <= 1e-10 * np.abs(K).max()
