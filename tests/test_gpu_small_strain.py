@@ -80,3 +80,49 @@ def test_small_strain_solve_vs_oracle(oracle, precision):
     assert np.abs(sig - om.gauss_stress()).max() / np.abs(om.gauss_stress()).max() < 1e-6
     assert np.abs(st["alpha"] - om.alpha).max() / max(np.abs(om.alpha).max(), 1e-300) < 1e-6
     assert np.array_equal(st["flags"], om.flags) and st["flags"].mean() > 0.2
+
+
+def _roller_cube(n, sigy0=250.0, strain=0.01):
+    """The reference's scaling cube (lagrangian/test/test_scaling.jl:16-26): rollers on
+    xmin/ymin/zmin, xmax pulled to `strain`, E = 210 GPa, H = 1 GPa, small strain."""
+    mesh = P.box_mesh(1.0, 1.0, 1.0, n, n, n)
+    mat = P.J2Material(E=210e3, nu=0.3, sigy0=sigy0, Hiso=1000.0)
+    M = P.Model(mesh, mat, element="small")
+    M.fix(P.on_face(mesh, "xmin"), "x")
+    M.fix(P.on_face(mesh, "ymin"), "y")
+    M.fix(P.on_face(mesh, "zmin"), "z")
+    M.prescribe(P.on_face(mesh, "xmax"), "x", strain)
+    return M
+
+
+def test_c1_cg_amg_matches_direct(oracle):
+    """test_scaling.jl:29-55 (C1): the plastic roller cube, 16^3, 12 steps, Newton
+    tol 1e-9: CG + AMG on the GPU against the direct (sparse LU) oracle, U and sigma
+    within 10 x 1e-8."""
+    M = _roller_cube(16)
+    res = M.solve(nsteps=12, tol=1e-9, maxiter=25)
+    assert res.converged
+    om = oracle.OracleModel(M.mesh.nodes, M.mesh.elements,
+                            oracle.J2Material(E=210e3, nu=0.3, sigy0=250.0, Hiso=1000.0), small=True)
+    om.dir_dofs, om.dir_vals, om.dir_ramp = list(M.dir_dofs), list(M.dir_vals), [bool(r) for r in M.dir_ramp]
+    ores = om.solve(nsteps=12, tol=1e-9)
+    assert ores["converged"]
+    assert rel(M.U, om.U) <= 1e-7
+    assert rel(P.gauss_stress(M).T, om.gauss_stress()) <= 1e-7
+
+
+def test_c2_mesh_independent_cg_count():
+    """test_scaling.jl:84-104 (C2): elastic roller cubes n = 8, 12, 16, 20, one step to
+    tol 1e-9; the largest CG count per Newton iteration grows with N at a log-log
+    slope <= 0.15 and stays <= 25."""
+    Ns, maxcg = [], []
+    for n in (8, 12, 16, 20):
+        M = _roller_cube(n, sigy0=1e9, strain=1e-3)
+        res = M.solve(nsteps=1, tol=1e-9, maxiter=25)
+        assert res.converged
+        Ns.append(M.ndof)
+        maxcg.append(max(res.cg_iters[0]))
+    lx, ly = np.log(Ns), np.log(maxcg)
+    slope = np.sum((lx - lx.mean()) * (ly - ly.mean())) / np.sum((lx - lx.mean()) ** 2)
+    assert slope <= 0.15, (Ns, maxcg, slope)
+    assert max(maxcg) <= 25, maxcg
