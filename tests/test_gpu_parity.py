@@ -221,3 +221,18 @@ def test_load_step_cutting_recovers_a_failed_increment():
     cut = M.solve(nsteps=2, tol=1e-8, maxiter=25, line_search=True, max_cuts=8)
     assert cut.converged and cut.stats["load_step_cuts"] > 0, cut.stats
     assert len(cut.iters) == 2
+
+
+def test_write_vtu_from_gpu_model(tmp_path):
+    """write_vtu(filename, model) (Visualization.jl:129-205) from a solved GPU model."""
+    import xml.etree.ElementTree as ET
+    from plasticity_b200 import visualization as V
+    w = W.config0(n=3, nsteps=2)
+    M = model_from(w)
+    assert M.solve(nsteps=2, tol=1e-10).converged
+    fn = V.write_vtu(str(tmp_path / "gpu_cube"), M)
+    root = ET.parse(fn).getroot()
+    arrs = {da.get("Name"): np.array(da.text.split(), float) for da in root.iter("DataArray") if da.get("Name")}
+    sig = P.gauss_stress(M).T.reshape(M.ne, 8, 6).mean(axis=1)
+    assert np.allclose(arrs["Stress"].reshape(M.ne, 6), sig, rtol=1e-15, atol=0)
+    assert np.allclose(arrs["Displacement"], M.U, rtol=0, atol=0)
