@@ -55,10 +55,17 @@ enum pfem_precision { PFEM_FP64 = 0, PFEM_MIXED = 1 };
 enum pfem_predictor { PFEM_PRED_PREVIOUS = 0, PFEM_PRED_EXTRAPOLATE = 1, PFEM_PRED_LEARNED = 2 };
 enum pfem_krylov { PFEM_KRYLOV_CG = 0, PFEM_KRYLOV_BICGSTAB = 1 };
 
-/* J2Material(; E, nu, sigy0, Hiso, Hkin), Materials.jl:82-108.  This path
- * supports linear isotropic hardening; Hkin must be 0. */
+/* J2Material(; E, nu, sigy0, Hiso, Hkin, sigsat, delta), Materials.jl:82-108.
+ * Isotropic hardening sigma_y(a) = sigy0 + (sigsat - sigy0)(1 - exp(-delta a)) +
+ * Hiso a (linear when delta = 0 or sigsat = sigy0), plus linear kinematic
+ * hardening Hkin.  sigsat = 0 stands for the reference's default sigsat = sigy0.
+ * Guards as the reference: E > 0, -1 < nu < 0.5, sigy0 > 0, Hiso >= 0,
+ * Hkin >= 0, sigsat >= sigy0, delta >= 0, and saturation together with Hkin > 0
+ * is rejected (PFEM_ERR_BAD_ARG).  With a per-element sigy0 the saturation
+ * amplitude stays sigsat - sigy0 of this struct. */
 typedef struct pfem_material {
   double E, nu, sigy0, Hiso, Hkin;
+  double sigsat, delta;
 } pfem_material;
 
 /* Keyword arguments of solve!, Solver.jl:419-422, and LinearSolveState,
@@ -87,6 +94,10 @@ typedef struct pfem_solve_opts {
                             element) is retried from the last converged state with half the
                             increment, at most max_cuts times per load step; 0 = the
                             reference (solve! stops, Solver.jl:455-466) */
+  double eta_first;      /* Eisenstat-Walker forcing only: while no load step of the path has
+                            converged yet (the first increment, from U = 0 and the full
+                            boundary-value jump), the inner tolerance is capped at eta_first;
+                            <= 0 = the reference's forcing term throughout */
 } pfem_solve_opts;
 
 typedef struct pfem_solve_result {
@@ -201,6 +212,13 @@ int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, d
 int pfem_set_state(pfem_ctx* ctx, const double* cpi, const double* alpha, const double* epsp);
 /* Overwrite U (host ndof) -- e.g. to evaluate a predictor guess. */
 int pfem_set_displacement(pfem_ctx* ctx, const double* U);
+/* Committed back stress beta (state_committed.beta, Model.jl:53-60), 6 x ngp
+ * column-major (physical-shear Voigt).  For the finite kinds it is the
+ * rotation-neutralised back stress of the reference configuration
+ * (FiniteStrain.jl:292-346).  get writes zeros when Hkin = 0; set needs
+ * Hkin > 0. */
+int pfem_get_back_stress(const pfem_ctx* ctx, double* beta);
+int pfem_set_back_stress(pfem_ctx* ctx, const double* beta);
 /* gauss_stress (Model.jl:188-208): Cauchy = tau / det F_gp (standard F). */
 int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma);
 

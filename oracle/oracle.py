@@ -50,10 +50,10 @@ def lib():
         L.or_return_map.restype = C.c_int
         L.or_return_map.argtypes = [_d, _d, _d, _d, C.c_double, _d, _d, _d, _d, _d]
         L.or_finite_update.restype = C.c_int
-        L.or_finite_update.argtypes = [_d, _d, _d, C.c_double, _d, _d, _d, _d, _d, _d]
+        L.or_finite_update.argtypes = [_d, _d, _d, C.c_double, _d, _d, _d, _d, _d, _d, _d, _d]
         L.or_element.restype = C.c_int
         L.or_element.argtypes = [C.c_int, _d, C.c_double, _d, _d, _d, _d, _d, _d, _d, _d, _d,
-                                 _d, _u8, _d]
+                                 _d, _d, _d, _u8, _d]
         L.or_pattern_nnz.restype = C.c_int64
         L.or_pattern_nnz.argtypes = [C.c_int64, C.c_int64, _i64]
         L.or_pattern_fill.restype = None
@@ -62,7 +62,7 @@ def lib():
         L.or_element_colors.argtypes = [C.c_int64, C.c_int64, _d, _i64]
         L.or_assemble.restype = C.c_int
         L.or_assemble.argtypes = [C.c_int, _d, _d, C.c_int64, C.c_int64, _d, _i64, _i64, _i64,
-                                  _d, _d, _d, _d, C.c_int, _d, _d, _d, _u8, C.c_int, _i64,
+                                  _d, _d, _d, _d, _d, C.c_int, _d, _d, _d, _u8, C.c_int, _i64,
                                   C.POINTER(C.c_int), _d]
         L.or_impose_dirichlet.restype = None
         L.or_impose_dirichlet.argtypes = [C.c_int64, _i64, _i64, _d, _d, C.c_int64, _i64, _d,
@@ -75,19 +75,33 @@ def _p(a, t=_d):
     return a.ctypes.data_as(t) if a is not None else None
 
 
-def _mat5(mat) -> np.ndarray:
-    return np.array([mat.E, mat.nu, mat.sigy0, mat.Hiso, mat.Hkin], dtype=np.float64)
+def _mat7(mat) -> np.ndarray:
+    return np.array([mat.E, mat.nu, mat.sigy0, mat.Hiso, mat.Hkin, mat.sigsat_value, mat.delta],
+                    dtype=np.float64)
 
 
 @dataclass
 class J2Material:
-    """J2Material (Materials.jl:68-108), linear isotropic (+ linear kinematic
-    for the small-strain return map only)."""
+    """J2Material (Materials.jl:68-108): linear or saturation (Voce) isotropic
+    hardening, sigma_y(a) = sigy0 + (sigsat - sigy0)(1 - exp(-delta a)) + Hiso a
+    (yield_stress, :117-118), plus linear kinematic hardening Hkin."""
     E: float
     nu: float
     sigy0: float
     Hiso: float = 0.0
     Hkin: float = 0.0
+    sigsat: float | None = None   # keyword default sigsat = sigy0
+    delta: float = 0.0
+
+    @property
+    def sigsat_value(self):
+        return self.sigy0 if self.sigsat is None else self.sigsat
+
+    def yield_stress(self, a):
+        return self.sigy0 + (self.sigsat_value - self.sigy0) * (1 - np.exp(-self.delta * a)) + self.Hiso * a
+
+    def yield_slope(self, a):
+        return self.delta * (self.sigsat_value - self.sigy0) * np.exp(-self.delta * a) + self.Hiso
 
     @property
     def G(self):
@@ -114,31 +128,34 @@ def return_map(mat, eps, epsp=None, beta=None, alpha=0.0):
     beta = np.zeros(6) if beta is None else np.ascontiguousarray(beta, dtype=np.float64)
     sig, ep2, b2, D = np.zeros(6), np.zeros(6), np.zeros(6), np.zeros(36)
     a2 = C.c_double(0.0)
-    m5 = _mat5(mat)
-    pl = lib().or_return_map(_p(m5), _p(eps), _p(epsp), _p(beta), alpha, _p(sig), _p(ep2),
+    m7 = _mat7(mat)
+    pl = lib().or_return_map(_p(m7), _p(eps), _p(epsp), _p(beta), alpha, _p(sig), _p(ep2),
                              _p(b2), C.byref(a2), _p(D))
     return sig, ep2, b2, a2.value, D.reshape(6, 6), pl
 
 
-def finite_update(mat, F, cpi=None, alpha=0.0):
+def finite_update(mat, F, cpi=None, alpha=0.0, beta=None):
     """finite_kinematics + finite_stress_update (+ dPdF), FiniteStrain.jl.
 
-    F is a 3x3 array.  Returns dict(tau, cpi_new, alpha, epsp_inc, D, A, plastic)
-    or raises ValueError when det F <= 0."""
+    F is a 3x3 array, beta the committed back stress in the reference
+    configuration (None = 0).  Returns dict(tau, cpi_new, alpha, beta, epsp_inc,
+    D, A, plastic) or raises ValueError when det F <= 0."""
     F9 = np.ascontiguousarray(np.asarray(F, dtype=np.float64).T.reshape(9))
     cpi = np.array([1, 1, 1, 0, 0, 0.0]) if cpi is None else np.ascontiguousarray(cpi, np.float64)
-    tau, cn, ei, D, A = np.zeros(6), np.zeros(6), np.zeros(6), np.zeros(36), np.zeros(81)
+    beta = np.zeros(6) if beta is None else np.ascontiguousarray(beta, np.float64)
+    tau, cn, bn, ei, D, A = (np.zeros(6), np.zeros(6), np.zeros(6), np.zeros(6), np.zeros(36),
+                             np.zeros(81))
     a2 = C.c_double(0.0)
-    m5 = _mat5(mat)
-    st = lib().or_finite_update(_p(m5), _p(F9), _p(cpi), alpha, _p(tau), _p(cn), C.byref(a2),
-                                _p(ei), _p(D), _p(A))
+    m7 = _mat7(mat)
+    st = lib().or_finite_update(_p(m7), _p(F9), _p(cpi), alpha, _p(beta), _p(tau), _p(cn),
+                                C.byref(a2), _p(bn), _p(ei), _p(D), _p(A))
     if st < 0:
         raise ValueError("det F <= 0")
-    return dict(tau=tau, cpi_new=cn, alpha=a2.value, epsp_inc=ei, D=D.reshape(6, 6),
+    return dict(tau=tau, cpi_new=cn, alpha=a2.value, beta=bn, epsp_inc=ei, D=D.reshape(6, 6),
                 A=A.reshape(9, 9), plastic=st)
 
 
-def element(fbar, mat, Xe, ue, cpi=None, alpha=None, sigy0=None):
+def element(fbar, mat, Xe, ue, cpi=None, alpha=None, sigy0=None, beta=None):
     """One Hex8 element: fbar 0 / 1 finite strain without / with F-bar
     (Elements.jl:405-494), 2 small strain (Elements.jl:323-360; cpi is then eps_p,
     tau is sigma).  Xe (8,3), ue (24,).  Returns dict."""
@@ -148,18 +165,20 @@ def element(fbar, mat, Xe, ue, cpi=None, alpha=None, sigy0=None):
         cpi = np.zeros(48) if int(fbar) == 2 else np.tile([1, 1, 1, 0, 0, 0.0], 8)
     cpi = np.ascontiguousarray(np.asarray(cpi, np.float64).reshape(48))
     alpha = np.zeros(8) if alpha is None else np.ascontiguousarray(alpha, np.float64)
-    Fe, Ke, tau, cn, an, ei = (np.zeros(24), np.zeros(576), np.zeros(48), np.zeros(48),
-                               np.zeros(8), np.zeros(48))
+    beta = np.zeros(48) if beta is None else np.ascontiguousarray(np.asarray(beta, np.float64).reshape(48))
+    Fe, Ke, tau, cn, an, bn, ei = (np.zeros(24), np.zeros(576), np.zeros(48), np.zeros(48),
+                                   np.zeros(8), np.zeros(48), np.zeros(48))
     fl = np.zeros(8, np.uint8)
     bJ = C.c_double(0.0)
-    m5 = _mat5(mat)
+    m7 = _mat7(mat)
     sy = mat.sigy0 if sigy0 is None else sigy0
-    st = lib().or_element(int(fbar), _p(m5), sy, _p(Xe), _p(ue), _p(cpi), _p(alpha), _p(Fe),
-                          _p(Ke), _p(tau), _p(cn), _p(an), _p(ei), _p(fl, _u8), C.byref(bJ))
+    st = lib().or_element(int(fbar), _p(m7), sy, _p(Xe), _p(ue), _p(cpi), _p(alpha), _p(beta),
+                          _p(Fe), _p(Ke), _p(tau), _p(cn), _p(an), _p(bn), _p(ei), _p(fl, _u8),
+                          C.byref(bJ))
     if st < 0:
         raise ElementInversionError(1, -st, bJ.value)
     return dict(Fe=Fe, Ke=Ke.reshape(24, 24), tau=tau.reshape(8, 6), cpi_new=cn.reshape(8, 6),
-                alpha=an, epsp_inc=ei.reshape(8, 6), flags=fl)
+                alpha=an, beta=bn.reshape(8, 6), epsp_inc=ei.reshape(8, 6), flags=fl)
 
 
 class ElementInversionError(Exception):
@@ -269,6 +288,7 @@ class OracleModel:
         if not self.small:
             self.cpi[:, :3] = 1.0
         self.alpha = np.zeros(ngp)
+        self.beta = np.zeros((ngp, 6))   # back stress (reference configuration for the finite kinds)
         self.epsp = np.zeros((ngp, 6))
         self.tau = np.zeros((ngp, 6))
         self.flags = np.zeros(ngp, np.uint8)
@@ -284,11 +304,12 @@ class OracleModel:
         alpha = self.alpha if alpha is None else alpha
         be = C.c_int64(0); bg = C.c_int(0); bJ = C.c_double(0)
         U = np.ascontiguousarray(U, np.float64)
-        m5 = _mat5(self.mat)
-        st = lib().or_assemble(2 if self.small else int(self.fbar), _p(m5), _p(self.sigy0_e), self.nn, self.ne,
+        m7 = _mat7(self.mat)
+        st = lib().or_assemble(2 if self.small else int(self.fbar), _p(m7), _p(self.sigy0_e), self.nn, self.ne,
                                _p(self._nodes_rm), _p(self._el_rm, _i64), _p(self.colptr, _i64),
                                _p(self.rowval, _i64), _p(U), _p(cpi), _p(alpha),
-                               _p(self.epsp), int(commit), _p(nz), _p(R), _p(tau),
+                               _p(self.epsp), _p(self.beta) if self.mat.Hkin > 0 else None,
+                               int(commit), _p(nz), _p(R), _p(tau),
                                _p(fl, _u8), self.nthreads, C.byref(be), C.byref(bg), C.byref(bJ))
         if st < 0:
             raise ElementInversionError(be.value, bg.value, bJ.value)

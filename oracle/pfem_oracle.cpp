@@ -53,13 +53,19 @@ void parallel_for(int64_t n, int nt, int64_t grain, Fn fn) {
 }
 
 struct Mat {
-  double E, nu, sigy0, Hiso, Hkin, G, K, lam;
+  double E, nu, sigy0, Hiso, Hkin, sigsat, delta, G, K, lam;
+  bool voce;  // saturation branch active (Materials.jl:201)
 };
 
-// J2Material constructor moduli, lagrangian/src/Materials.jl:104-107.
-Mat make_mat(const double* m5) {
+// J2Material constructor moduli, lagrangian/src/Materials.jl:82-108.  m7 =
+// (E, nu, sigy0, Hiso, Hkin, sigsat, delta); sigsat <= 0 stands for the
+// keyword default sigsat = sigy0.
+Mat make_mat(const double* m7) {
   Mat m;
-  m.E = m5[0]; m.nu = m5[1]; m.sigy0 = m5[2]; m.Hiso = m5[3]; m.Hkin = m5[4];
+  m.E = m7[0]; m.nu = m7[1]; m.sigy0 = m7[2]; m.Hiso = m7[3]; m.Hkin = m7[4];
+  m.sigsat = m7[5] > 0 ? m7[5] : m7[2];
+  m.delta = m7[6];
+  m.voce = m.delta > 0 && m.sigsat > m.sigy0;
   m.G = m.E / (2.0 * (1.0 + m.nu));
   m.K = m.E / (3.0 * (1.0 - 2.0 * m.nu));
   m.lam = m.E * m.nu / ((1.0 + m.nu) * (1.0 - 2.0 * m.nu));
@@ -81,8 +87,19 @@ double devnorm(const double s[6]) {
                    2.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5]));
 }
 
-// return_map, linear-hardening branch, Materials.jl:159-250 (yield_stress
-// :117-118 and yield_slope :126-127 with sigma_sat == sigma_y0).
+// yield_stress, Materials.jl:117-118.  sy0 is the element's initial yield
+// stress (the material's unless a per-element value is given); the saturation
+// amplitude is the material's sigsat - sigy0.
+double yield_stress(const Mat& m, double sy0, double a) {
+  return sy0 + (m.sigsat - m.sigy0) * (1.0 - std::exp(-m.delta * a)) + m.Hiso * a;
+}
+// yield_slope, Materials.jl:126-127.
+double yield_slope(const Mat& m, double a) {
+  return m.delta * (m.sigsat - m.sigy0) * std::exp(-m.delta * a) + m.Hiso;
+}
+
+// return_map, Materials.jl:159-250: linear branch (closed-form dgamma, :218)
+// or the saturation branch (scalar local Newton on dgamma, :201-213).
 // Returns 1 for the plastic branch (f_tr > 0), 0 for elastic.
 int return_map(const Mat& m, double sigy0, const double eps[6], const double epsp_n[6],
                const double beta_n[6], double alpha_n, double sig[6], double epsp_new[6],
@@ -102,7 +119,7 @@ int return_map(const Mat& m, double sigy0, const double eps[6], const double eps
   for (int i = 0; i < 6; ++i) xi[i] = st[i] - (i < 3 ? p : 0.0) - beta_n[i];
   const double nrm = devnorm(xi);
   const double q = std::sqrt(1.5) * nrm;
-  const double ftr = q - (sigy0 + m.Hiso * alpha_n);
+  const double ftr = m.voce ? q - yield_stress(m, sigy0, alpha_n) : q - (sigy0 + m.Hiso * alpha_n);
   if (ftr_out) *ftr_out = ftr;
   if (ftr <= 0.0) {
     for (int i = 0; i < 6; ++i) {
@@ -116,13 +133,25 @@ int return_map(const Mat& m, double sigy0, const double eps[6], const double eps
   double nh[6];
   for (int i = 0; i < 6; ++i) nh[i] = xi[i] / nrm;
   const double G = m.G;
-  const double dg = ftr / (3.0 * G + m.Hiso + m.Hkin);
+  double dg;
+  if (m.voce) {
+    dg = ftr / (3.0 * G + m.Hkin + yield_slope(m, alpha_n));
+    for (int it = 0; it < 50; ++it) {
+      const double Hp = yield_slope(m, alpha_n + dg);
+      const double r = q - (3.0 * G + m.Hkin) * dg - yield_stress(m, sigy0, alpha_n + dg);
+      const double d = r / (3.0 * G + m.Hkin + Hp);
+      dg += d;
+      if (std::fabs(d) <= 1e-13 * (dg + 1e-14)) break;
+    }
+  } else {
+    dg = ftr / (3.0 * G + m.Hiso + m.Hkin);
+  }
   for (int i = 0; i < 6; ++i) sig[i] = st[i] - (2.0 * G * dg * s32) * nh[i];
   for (int i = 0; i < 6; ++i)
     epsp_new[i] = epsp_n[i] + (dg * s32) * (i < 3 ? nh[i] : 2.0 * nh[i]);
   for (int i = 0; i < 6; ++i) beta_new[i] = beta_n[i] + (2.0 / 3.0) * m.Hkin * (dg * s32) * nh[i];
   *alpha_new = alpha_n + dg;
-  const double Hp = m.Hiso;
+  const double Hp = m.voce ? yield_slope(m, *alpha_new) : m.Hiso;
   const double b0 = 2.0 * G * dg / q;
   const double g0 = 2.0 * G / (3.0 * G + m.Hkin + Hp);
   for (int i = 0; i < 6; ++i)
@@ -263,19 +292,128 @@ Kin finite_kinematics(const double F[3][3], const double cpi_v[6]) {
   return k;
 }
 
+// Right polar decomposition F = R U, polar_RU (FiniteStrain.jl:194-210):
+// U = (F^T F)^(1/2) through the eigenbasis V of F^T F (eigenvalues floored at
+// 0), R = F U^-1.  mu receives U's eigenvalues, V its eigenvectors (columns),
+// which dR_polar reuses (the reference decomposes U again; it has the same
+// eigenbasis and eigenvalues).
+void polar_RU(const double F[3][3], double R[3][3], double Um[3][3], double V[3][3], double mu[3]) {
+  double Ft[3][3], C[3][3];
+  tr3(F, Ft);
+  mul3(Ft, F, C);
+  double w[3];
+  eig3(C, w, V);
+  double isq[3];
+  for (int A = 0; A < 3; ++A) {
+    mu[A] = std::sqrt(std::max(w[A], 0.0));
+    isq[A] = mu[A] > 0 ? 1.0 / mu[A] : 0.0;
+  }
+  double Ui[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double u = 0.0, ui = 0.0;
+      for (int A = 0; A < 3; ++A) {
+        u += V[i][A] * mu[A] * V[j][A];
+        ui += V[i][A] * isq[A] * V[j][A];
+      }
+      Um[i][j] = u;
+      Ui[i][j] = ui;
+    }
+  mul3(F, Ui, R);
+}
+
+// dR_polar (FiniteStrain.jl:220-233): Omega U + U Omega = R^T dF - dF^T R solved
+// in U's eigenbasis, dR = R Omega.
+void dR_polar(const double R[3][3], const double V[3][3], const double mu[3], const double dF[3][3],
+              double dR[3][3]) {
+  double Rt[3][3], A[3][3], rhs[3][3];
+  tr3(R, Rt);
+  mul3(Rt, dF, A);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) rhs[i][j] = A[i][j] - A[j][i];
+  double Vt[3][3], T[3][3], rb[3][3];
+  tr3(V, Vt);
+  mul3(Vt, rhs, T);
+  mul3(T, V, rb);
+  double Ob[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Ob[i][j] = rb[i][j] / (mu[i] + mu[j]);
+  double O[3][3];
+  mul3(V, Ob, T);
+  mul3(T, Vt, O);
+  mul3(R, O, dR);
+}
+
+// dtau_dbeta (FiniteStrain.jl:250-268), row-major 6x6: zero in the elastic
+// branch, else a I + xi (x) g with g = (da/dnrm / nrm) W xi.
+void dtau_dbeta(const Mat& m, double sy0, const double eps_tr[6], const double beta_sp[6], double alpha_n,
+                double out[36]) {
+  std::memset(out, 0, 36 * sizeof(double));
+  const double G = m.G, H = m.Hiso + m.Hkin, s32 = std::sqrt(1.5);
+  double C[36];
+  cmat(m, C);
+  double st[6];
+  for (int i = 0; i < 6; ++i) {
+    double t = 0.0;
+    for (int j = 0; j < 6; ++j) t += C[i * 6 + j] * eps_tr[j];
+    st[i] = t;
+  }
+  const double p = (st[0] + st[1] + st[2]) / 3.0;
+  double xi[6];
+  for (int i = 0; i < 6; ++i) xi[i] = st[i] - (i < 3 ? p : 0.0) - beta_sp[i];
+  const double nrm = devnorm(xi);
+  const double Y = sy0 + m.Hiso * alpha_n;
+  const double f = s32 * nrm - Y;
+  if (f <= 0.0) return;
+  const double dg = f / (3.0 * G + H);
+  const double a = 2.0 * G * s32 * dg / nrm;
+  const double da = 2.0 * G * s32 / (3.0 * G + H) * (Y / (nrm * nrm));
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j)
+      out[i * 6 + j] = (i == j ? a : 0.0) + xi[i] * (da / nrm) * (j < 3 ? 1.0 : 2.0) * xi[j];
+}
+
 struct Upd {
   double tau[6], epsp_inc[6], alpha_new, D[36], cpi_new[6], ftr;
+  double beta_ref_new[6], beta_sp[6], R[3][3], Um[3][3], V[3][3], mu[3];
   int plastic;
 };
 
-// finite_stress_update for Hkin = 0 (FiniteStrain.jl:292-346, the branch at
-// :316 with R = U = I and beta_sp = 0).
-Upd finite_stress_update(const Mat& m, double sigy0, const Kin& k, double alpha_n) {
+// finite_stress_update (FiniteStrain.jl:292-346).  With Hkin > 0 the back
+// stress is stored in the reference configuration: beta_sp = R beta_ref R^T
+// enters the return map and the update is pulled back, beta_ref_new =
+// R^T beta_sp_new R (:316-324).  With Hkin = 0, R = U = I and beta_sp = 0.
+Upd finite_stress_update(const Mat& m, double sigy0, const Kin& k, const double F[3][3], double alpha_n,
+                         const double* beta_ref_n) {
   Upd u;
   const double Z6[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) u.R[i][j] = u.Um[i][j] = u.V[i][j] = (i == j) ? 1.0 : 0.0;
+  u.mu[0] = u.mu[1] = u.mu[2] = 1.0;
+  std::memset(u.beta_sp, 0, sizeof(u.beta_sp));
+  const bool kin = m.Hkin > 0;
+  if (kin) {
+    polar_RU(F, u.R, u.Um, u.V, u.mu);
+    double B[3][3], T[3][3], Rt[3][3], S[3][3];
+    v2s(beta_ref_n, B);
+    tr3(u.R, Rt);
+    mul3(u.R, B, T);
+    mul3(T, Rt, S);
+    s2v(S, u.beta_sp);
+  }
   double beta_new[6];
-  u.plastic = return_map(m, sigy0, k.eps_tr, Z6, Z6, alpha_n, u.tau, u.epsp_inc, beta_new,
+  u.plastic = return_map(m, sigy0, k.eps_tr, Z6, u.beta_sp, alpha_n, u.tau, u.epsp_inc, beta_new,
                          &u.alpha_new, u.D, &u.ftr);
+  if (kin) {
+    double B[3][3], T[3][3], Rt[3][3], S[3][3];
+    v2s(beta_new, B);
+    tr3(u.R, Rt);
+    mul3(Rt, B, T);
+    mul3(T, u.R, S);
+    s2v(S, u.beta_ref_new);
+  } else {
+    std::memcpy(u.beta_ref_new, beta_new, sizeof(beta_new));
+  }
   double ee[6];
   for (int i = 0; i < 6; ++i) ee[i] = k.eps_tr[i] - u.epsp_inc[i];
   double E2[3][3] = {{2 * ee[0], ee[3], ee[5]}, {ee[3], 2 * ee[1], ee[4]}, {ee[5], ee[4], 2 * ee[2]}};
@@ -317,10 +455,14 @@ void dhalflog_contract(const double Q[3][3], const double b[3], const double H[3
   mul3(T, Qt, out);
 }
 
-// dPdF for Hkin = 0 (FiniteStrain.jl:503-547; the kinematic term at :532-536
-// vanishes).  A9 is 9x9 row-major with both indices column-major F/P order.
+// dPdF (FiniteStrain.jl:503-547).  A9 is 9x9 row-major with both indices
+// column-major F/P order.  kin (non-null) carries the kinematic-hardening
+// coupling dtau/dbeta_sp . dbeta_sp/dF through the polar rotation (:532-536).
+struct KinTerm {
+  double Bref[3][3], R[3][3], V[3][3], mu[3], dtdb[36];
+};
 void dPdF(const Kin& k, const double cpi_v[6], const double D[36], const double tau_v[6],
-          const double F[3][3], double A9[81]) {
+          const double F[3][3], double A9[81], const KinTerm* kin = nullptr) {
   double Cpi[3][3], tau[3][3], FinvT[3][3], Ft[3][3];
   v2s(cpi_v, Cpi);
   v2s(tau_v, tau);
@@ -347,6 +489,25 @@ void dPdF(const Kin& k, const double cpi_v[6], const double D[36], const double 
       double s = 0.0;
       for (int j = 0; j < 6; ++j) s += D[i * 6 + j] * dev[j];
       dtv[i] = s;
+    }
+    if (kin) {
+      double dR[3][3], Rt[3][3], dRt[3][3], T1[3][3], T2[3][3], T3[3][3], T4[3][3], db[3][3];
+      dR_polar(kin->R, kin->V, kin->mu, dF, dR);
+      tr3(kin->R, Rt);
+      tr3(dR, dRt);
+      mul3(dR, kin->Bref, T1);
+      mul3(T1, Rt, T2);
+      mul3(kin->R, kin->Bref, T3);
+      mul3(T3, dRt, T4);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) db[i][j] = T2[i][j] + T4[i][j];
+      double dbv[6];
+      s2v(db, dbv);
+      for (int i = 0; i < 6; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < 6; ++j) s += kin->dtdb[i * 6 + j] * dbv[j];
+        dtv[i] += s;
+      }
     }
     double dt[3][3];
     v2s(dtv, dt);
@@ -434,32 +595,48 @@ extern "C" {
 
 // ---- material / kinematics entry points (reference tests T1-T7, F3-F5) ----
 
-int or_return_map(const double* mat5, const double* eps6, const double* epsp6,
+int or_return_map(const double* mat7, const double* eps6, const double* epsp6,
                   const double* beta6, double alpha_n, double* sig6, double* epsp_new6,
                   double* beta_new6, double* alpha_new, double* D36) {
-  Mat m = make_mat(mat5);
+  Mat m = make_mat(mat7);
   return return_map(m, m.sigy0, eps6, epsp6, beta6, alpha_n, sig6, epsp_new6, beta_new6,
                     alpha_new, D36, nullptr);
 }
 
-// F given column-major 9 (F[j*3+i] = F_ij).  Returns -1 when det F <= 0,
-// else the plastic flag.
-int or_finite_update(const double* mat5, const double* F9, const double* cpi6, double alpha_n,
-                     double* tau6, double* cpi_new6, double* alpha_new, double* epsp_inc6,
-                     double* D36, double* A81) {
-  Mat m = make_mat(mat5);
+// F given column-major 9 (F[j*3+i] = F_ij).  beta6: committed back stress in
+// the reference configuration (null = 0).  Returns -1 when det F <= 0, else
+// the plastic flag.
+int or_finite_update(const double* mat7, const double* F9, const double* cpi6, double alpha_n,
+                     const double* beta6, double* tau6, double* cpi_new6, double* alpha_new,
+                     double* beta_new6, double* epsp_inc6, double* D36, double* A81) {
+  Mat m = make_mat(mat7);
   double F[3][3];
   for (int j = 0; j < 3; ++j)
     for (int i = 0; i < 3; ++i) F[i][j] = F9[j * 3 + i];
   Kin k = finite_kinematics(F, cpi6);
   if (!k.ok) return -1;
-  Upd u = finite_stress_update(m, m.sigy0, k, alpha_n);
+  const double Z6[6] = {0, 0, 0, 0, 0, 0};
+  const double* bn = beta6 ? beta6 : Z6;
+  Upd u = finite_stress_update(m, m.sigy0, k, F, alpha_n, bn);
   std::memcpy(tau6, u.tau, sizeof(u.tau));
   std::memcpy(cpi_new6, u.cpi_new, sizeof(u.cpi_new));
   *alpha_new = u.alpha_new;
+  if (beta_new6) std::memcpy(beta_new6, u.beta_ref_new, sizeof(u.beta_ref_new));
   if (epsp_inc6) std::memcpy(epsp_inc6, u.epsp_inc, sizeof(u.epsp_inc));
   if (D36) std::memcpy(D36, u.D, sizeof(u.D));
-  if (A81) dPdF(k, cpi6, u.D, u.tau, F, A81);
+  if (A81) {
+    if (m.Hkin > 0) {
+      KinTerm kt;
+      v2s(bn, kt.Bref);
+      std::memcpy(kt.R, u.R, sizeof(kt.R));
+      std::memcpy(kt.V, u.V, sizeof(kt.V));
+      std::memcpy(kt.mu, u.mu, sizeof(kt.mu));
+      dtau_dbeta(m, m.sigy0, k.eps_tr, u.beta_sp, alpha_n, kt.dtdb);
+      dPdF(k, cpi6, u.D, u.tau, F, A81, &kt);
+    } else {
+      dPdF(k, cpi6, u.D, u.tau, F, A81);
+    }
+  }
   return u.plastic;
 }
 
@@ -469,25 +646,28 @@ int or_finite_update(const double* mat5, const double* F9, const double* cpi6, d
 // F-bar chain of _fbar_Geff, Elements.jl:524-531; fbar = 2: the small-strain
 // element_force_tangent!, Elements.jl:323-360 (state slot = eps_p, tau = sigma).
 //   Xe24: node-major coordinates (a*3 + d); ue24 node-major displacements.
-//   cpi48 / alpha8: committed state per Gauss point (g*6 + c, g).
+//   cpi48 / alpha8 / beta48: committed state per Gauss point (g*6 + c, g);
+//   beta48 (null = 0) is the back stress (reference configuration for the
+//   finite kinds), beta_new48 (nullable) receives its update.
 //   Ke576 row-major 24x24.  tau48 Kirchhoff stress per GP.  flags8 = f_tr>0.
 // Returns 0, or -(g+1) for the first inverted Gauss point g (J in *badJ).
-int or_element(int fbar, const double* mat5, double sigy0, const double* Xe24,
-               const double* ue24, const double* cpi48, const double* alpha8, double* Fe24,
-               double* Ke576, double* tau48, double* cpi_new48, double* alpha_new8,
-               double* epsp_inc48, unsigned char* flags8, double* badJ) {
-  Mat m = make_mat(mat5);
+int or_element(int fbar, const double* mat7, double sigy0, const double* Xe24,
+               const double* ue24, const double* cpi48, const double* alpha8, const double* beta48,
+               double* Fe24, double* Ke576, double* tau48, double* cpi_new48, double* alpha_new8,
+               double* beta_new48, double* epsp_inc48, unsigned char* flags8, double* badJ) {
+  Mat m = make_mat(mat7);
+  static const double Z48[48] = {0};
+  if (!beta48) beta48 = Z48;
   double Xe[8][3];
   for (int a = 0; a < 8; ++a)
     for (int d = 0; d < 3; ++d) Xe[a][d] = Xe24[a * 3 + d];
   if (fbar == 2) {
     // Small strain: element_force_tangent!, Elements.jl:323-360, with bmatrix
-    // :97-117 and return_map (Hkin = 0, so beta stays zero).  The state slot
-    // cpi48 carries eps_p (6 per GP, engineering shear), tau48 receives sigma.
+    // :97-117 and return_map.  The state slot cpi48 carries eps_p (6 per GP,
+    // engineering shear), tau48 receives sigma.
     const double g = 1.0 / std::sqrt(3.0);
     std::memset(Fe24, 0, 24 * sizeof(double));
     std::memset(Ke576, 0, 576 * sizeof(double));
-    const double beta0[6] = {0, 0, 0, 0, 0, 0};
     for (int gp = 0; gp < 8; ++gp) {
       const double xi[3] = {GSGN[gp][0] * g, GSGN[gp][1] * g, GSGN[gp][2] * g};
       double dNdX[8][3];
@@ -510,8 +690,9 @@ int or_element(int fbar, const double* mat5, double sigy0, const double* Xe24,
         eps[r] = t;
       }
       double sig[6], ep_new[6], b_new[6], a_new, D[36];
-      const int pl = return_map(m, sigy0, eps, cpi48 + gp * 6, beta0, alpha8[gp], sig, ep_new, b_new, &a_new,
-                                D, nullptr);
+      const int pl = return_map(m, sigy0, eps, cpi48 + gp * 6, beta48 + gp * 6, alpha8[gp], sig, ep_new, b_new,
+                                &a_new, D, nullptr);
+      if (beta_new48) std::memcpy(beta_new48 + gp * 6, b_new, sizeof(b_new));
       for (int c = 0; c < 24; ++c) {
         double t = 0.0;
         for (int r = 0; r < 6; ++r) t += B[r * 24 + c] * sig[r];
@@ -575,7 +756,7 @@ int or_element(int fbar, const double* mat5, double sigy0, const double* Xe24,
       if (badJ) *badJ = k.J;
       return -(gp + 1);
     }
-    Upd u = finite_stress_update(m, sigy0, k, alpha8[gp]);
+    Upd u = finite_stress_update(m, sigy0, k, Fb, alpha8[gp], beta48 + gp * 6);
     double Gm[9 * 24];
     Gmatrix(dNdX, Gm);
     double tau[3][3], FinvT[3][3], P[3][3];
@@ -585,7 +766,17 @@ int or_element(int fbar, const double* mat5, double sigy0, const double* Xe24,
     double Pv[9];
     p9(P, Pv);
     double A[81];
-    dPdF(k, cpi48 + gp * 6, u.D, u.tau, Fb, A);
+    if (m.Hkin > 0) {
+      KinTerm kt;
+      v2s(beta48 + gp * 6, kt.Bref);
+      std::memcpy(kt.R, u.R, sizeof(kt.R));
+      std::memcpy(kt.V, u.V, sizeof(kt.V));
+      std::memcpy(kt.mu, u.mu, sizeof(kt.mu));
+      dtau_dbeta(m, sigy0, k.eps_tr, u.beta_sp, alpha8[gp], kt.dtdb);
+      dPdF(k, cpi48 + gp * 6, u.D, u.tau, Fb, A, &kt);
+    } else {
+      dPdF(k, cpi48 + gp * 6, u.D, u.tau, Fb, A);
+    }
     for (int c = 0; c < 24; ++c) {
       double s = 0.0;
       for (int r = 0; r < 9; ++r) s += Gm[r * 24 + c] * Pv[r];
@@ -627,6 +818,7 @@ int or_element(int fbar, const double* mat5, double sigy0, const double* Xe24,
     if (tau48) std::memcpy(tau48 + gp * 6, u.tau, 6 * sizeof(double));
     if (cpi_new48) std::memcpy(cpi_new48 + gp * 6, u.cpi_new, 6 * sizeof(double));
     if (alpha_new8) alpha_new8[gp] = u.alpha_new;
+    if (beta_new48) std::memcpy(beta_new48 + gp * 6, u.beta_ref_new, 6 * sizeof(double));
     if (epsp_inc48) std::memcpy(epsp_inc48 + gp * 6, u.epsp_inc, 6 * sizeof(double));
     if (flags8) flags8[gp] = (unsigned char)u.plastic;
   }
@@ -724,10 +916,10 @@ int or_element_colors(int64_t nn, int64_t ne, const double* nodes, int64_t* colo
 // independent of the thread count.  State arrays are 6 x ngp column-major.
 // commit != 0 writes cpi/alpha/epsp in place (Elements.jl:483-491).
 // Returns 0, or -1 on an inverted element (bad_e 1-based, bad_g 1-based, badJ).
-int or_assemble(int fbar, const double* mat5, const double* sigy0_e, int64_t nn, int64_t ne,
+int or_assemble(int fbar, const double* mat7, const double* sigy0_e, int64_t nn, int64_t ne,
                 const double* nodes, const int64_t* elem, const int64_t* colptr,
                 const int64_t* rowval, const double* U, double* cpi, double* alpha,
-                double* epsp, int commit, double* nzval, double* R, double* tau,
+                double* epsp, double* beta, int commit, double* nzval, double* R, double* tau,
                 unsigned char* flags, int nthreads, int64_t* bad_e, int* bad_g, double* badJ) {
   const int64_t ndof = 3 * nn;
   const int64_t nnz = colptr[ndof] - 1;
@@ -735,7 +927,7 @@ int or_assemble(int fbar, const double* mat5, const double* sigy0_e, int64_t nn,
   std::fill(R, R + ndof, 0.0);
   const int64_t CH = 2048;
   std::vector<double> Fe(CH * 24), Ke(CH * 576);
-  std::vector<double> cnew(CH * 48), anew(CH * 8), pinc(CH * 48);
+  std::vector<double> cnew(CH * 48), anew(CH * 8), pinc(CH * 48), bnew(beta ? CH * 48 : 0);
   std::vector<int> st(CH);
   std::vector<double> sJ(CH);
   const int nt = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -751,10 +943,11 @@ int or_assemble(int fbar, const double* mat5, const double* sigy0_e, int64_t nn,
           ue[a * 3 + d] = U[nd * 3 + d];
         }
       }
-      const double sy = sigy0_e ? sigy0_e[e] : mat5[2];
-      st[q] = or_element(fbar, mat5, sy, Xe, ue, cpi + e * 48, alpha + e * 8, &Fe[q * 24],
-                         &Ke[q * 576], tau ? tau + e * 48 : nullptr, &cnew[q * 48],
-                         &anew[q * 8], &pinc[q * 48], flags ? flags + e * 8 : nullptr, &sJ[q]);
+      const double sy = sigy0_e ? sigy0_e[e] : mat7[2];
+      st[q] = or_element(fbar, mat7, sy, Xe, ue, cpi + e * 48, alpha + e * 8, beta ? beta + e * 48 : nullptr,
+                         &Fe[q * 24], &Ke[q * 576], tau ? tau + e * 48 : nullptr, &cnew[q * 48],
+                         &anew[q * 8], beta ? &bnew[q * 48] : nullptr, &pinc[q * 48],
+                         flags ? flags + e * 8 : nullptr, &sJ[q]);
     });
     for (int64_t e = e0; e < e1; ++e) {
       const int64_t q = e - e0;
@@ -785,6 +978,7 @@ int or_assemble(int fbar, const double* mat5, const double* sigy0_e, int64_t nn,
       if (commit) {
         std::memcpy(cpi + e * 48, &cnew[q * 48], 48 * sizeof(double));
         std::memcpy(alpha + e * 8, &anew[q * 8], 8 * sizeof(double));
+        if (beta) std::memcpy(beta + e * 48, &bnew[q * 48], 48 * sizeof(double));
         if (epsp)
           for (int i = 0; i < 48; ++i) epsp[e * 48 + i] += pinc[q * 48 + i];
       }

@@ -34,7 +34,8 @@ PFEM_KRYLOV_BICGSTAB = 1
 
 class Material(C.Structure):
     _fields_ = [("E", C.c_double), ("nu", C.c_double), ("sigy0", C.c_double),
-                ("Hiso", C.c_double), ("Hkin", C.c_double)]
+                ("Hiso", C.c_double), ("Hkin", C.c_double), ("sigsat", C.c_double),
+                ("delta", C.c_double)]
 
 
 class SolveOpts(C.Structure):
@@ -43,7 +44,8 @@ class SolveOpts(C.Structure):
                 ("eta_min", C.c_double), ("eta_max", C.c_double), ("ew_gamma", C.c_double),
                 ("ew_alpha", C.c_double), ("krylov_itmax", C.c_int32), ("predictor", C.c_int32),
                 ("amg_rebuild", C.c_int32), ("cheb_degree", C.c_int32), ("verbose", C.c_int32),
-                ("line_search", C.c_int32), ("predictor_smooth", C.c_int32), ("max_cuts", C.c_int32)]
+                ("line_search", C.c_int32), ("predictor_smooth", C.c_int32), ("max_cuts", C.c_int32),
+                ("eta_first", C.c_double)]
 
 
 class SolveResultC(C.Structure):
@@ -84,6 +86,8 @@ SIGNATURES = {
     "pfem_amg_dense": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d, _i64]),
     "pfem_get_state": (C.c_int, [_ctx, _d, _d, _d, _d, _d, _u8]),
     "pfem_set_state": (C.c_int, [_ctx, _d, _d, _d]),
+    "pfem_get_back_stress": (C.c_int, [_ctx, _d]),
+    "pfem_set_back_stress": (C.c_int, [_ctx, _d]),
     "pfem_set_displacement": (C.c_int, [_ctx, _d]),
     "pfem_gauss_stress": (C.c_int, [_ctx, _d]),
     "pfem_profile": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d]),

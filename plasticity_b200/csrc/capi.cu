@@ -100,6 +100,8 @@ struct pfem_ctx {
   int* dColorList = nullptr;
   int* dAllElems = nullptr;
   double *dCpi = nullptr, *dAlpha = nullptr, *dEpsp = nullptr, *dTau = nullptr;
+  double* dBeta = nullptr;  // 6 x ngp committed back stress, kinematic hardening only
+  int hard = HARD_LINEAR;   // hardening law of the element kernels
   uint8_t* dFlags = nullptr;
   double *dU = nullptr, *dR = nullptr, *dDg = nullptr, *dUprev = nullptr, *dUprev2 = nullptr;
   double* dUprev3 = nullptr;
@@ -1033,11 +1035,11 @@ int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
   if (commit) {
     ElemArgs<double> a{};
     a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
-    a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+    a.epsp = ctx->dEpsp; a.beta = ctx->dBeta; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
     a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
-    if (small) launch_element_small<double>(a, ctx->dAllElems, (int)ctx->ne, true, st);
-    else launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, true, fbar, st);
+    if (small) launch_element_small<double>(a, ctx->dAllElems, (int)ctx->ne, true, ctx->hard, st);
+    else launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, true, fbar, ctx->hard, st);
     CKL();
     return PFEM_OK;
   }
@@ -1047,27 +1049,27 @@ int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
     CK(cudaMemsetAsync(ctx->dK64, 0, (size_t)ctx->nnzb * 9 * sizeof(double), st));
     ElemArgs<double> a{};
     a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
-    a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+    a.epsp = ctx->dEpsp; a.beta = ctx->dBeta; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
     a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
     for (int c = 0; c < nc; ++c) {
       const int* cl = ctx->dColorList + ctx->color_ptr[c];
       const int cn = ctx->color_ptr[c + 1] - ctx->color_ptr[c];
-      if (small) launch_element_small<double>(a, cl, cn, false, st);
-      else launch_element_color<double>(a, cl, cn, false, fbar, st);
+      if (small) launch_element_small<double>(a, cl, cn, false, ctx->hard, st);
+      else launch_element_color<double>(a, cl, cn, false, fbar, ctx->hard, st);
     }
   } else {
     CK(cudaMemsetAsync(ctx->dK32, 0, (size_t)ctx->nnzb * 9 * sizeof(float), st));
     ElemArgs<float> a{};
     a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
-    a.epsp = ctx->dEpsp; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+    a.epsp = ctx->dEpsp; a.beta = ctx->dBeta; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
     a.R = ctx->dR; a.Kval = ctx->dK32; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
     for (int c = 0; c < nc; ++c) {
       const int* cl = ctx->dColorList + ctx->color_ptr[c];
       const int cn = ctx->color_ptr[c + 1] - ctx->color_ptr[c];
-      if (small) launch_element_small<float>(a, cl, cn, false, st);
-      else launch_element_color<float>(a, cl, cn, false, fbar, st);
+      if (small) launch_element_small<float>(a, cl, cn, false, ctx->hard, st);
+      else launch_element_color<float>(a, cl, cn, false, fbar, ctx->hard, st);
     }
   }
   CKL();
@@ -1208,6 +1210,10 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     // After a backtracked step the iterate is outside Newton's fast region; a
     // loose inner solve there gives poor directions, so tighten it.
     if (damped) eta = std::min(eta, 1e-3);
+    // The first increment starts from U = 0 with the whole boundary-value jump; a loose
+    // first direction there sends the line search into a long damped sequence
+    // (measured at 64^3-100^3: 33-50 Newton iterations at eta_max = 0.1, 5-18 at 1e-2).
+    if (o->lin_rtol <= 0 && o->eta_first > 0 && ctx->steps_taken == 0) eta = std::min(eta, o->eta_first);
     const bool rebuild = first || o->amg_rebuild;
     first = false;
     int kits = 0;
@@ -1257,12 +1263,14 @@ __global__ void extrap_kernel(long long n, double f, const double* __restrict__ 
     u[i] = u1[i] + f * (u1[i] - u2[i]);
 }
 
-__global__ void init_state_kernel(long long ngp, double* cpi, double* alpha, double* epsp, double* tau) {
+__global__ void init_state_kernel(long long ngp, double* cpi, double* alpha, double* epsp, double* tau,
+                                  double* beta) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ngp; i += (long long)gridDim.x * blockDim.x) {
     for (int c = 0; c < 6; ++c) {
       cpi[c * ngp + i] = c < 3 ? 1.0 : 0.0;
       epsp[c * ngp + i] = 0.0;
       tau[c * ngp + i] = 0.0;
+      if (beta) beta[c * ngp + i] = 0.0;
     }
     alpha[i] = 0.0;
   }
@@ -1361,6 +1369,7 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->line_search = 0;
   o->predictor_smooth = 16;
   o->max_cuts = 0;
+  o->eta_first = 1e-2;
 }
 
 const char* pfem_last_error(const pfem_ctx* ctx) {
@@ -1372,13 +1381,20 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
                 int32_t kind, const pfem_material* m, const double* sigy0_e, int32_t device) {
   if (!out || !nodes || !elements || !m || nn <= 0 || ne <= 0) return PFEM_ERR_BAD_ARG;
   *out = nullptr;
-  // J2Material guards, Materials.jl:90-103
+  // J2Material guards, Materials.jl:90-103 (sigsat == 0 stands for the keyword
+  // default sigsat = sigy0)
   if (!(m->E > 0) || !(m->nu > -1 && m->nu < 0.5) || !(m->sigy0 > 0) || !(m->Hiso >= 0) || !(m->Hkin >= 0)) {
     g_cuda_err = "invalid material parameters (E>0, -1<nu<0.5, sigy0>0, Hiso>=0, Hkin>=0)";
     return PFEM_ERR_BAD_ARG;
   }
-  if (m->Hkin != 0.0) {
-    g_cuda_err = "this path implements linear isotropic hardening only (Hkin must be 0)";
+  const double sigsat = m->sigsat == 0.0 ? m->sigy0 : m->sigsat;
+  if (!(sigsat >= m->sigy0) || !(m->delta >= 0)) {
+    g_cuda_err = "invalid saturation parameters (sigsat >= sigy0, delta >= 0)";
+    return PFEM_ERR_BAD_ARG;
+  }
+  const bool voce = m->delta > 0 && sigsat > m->sigy0;
+  if (voce && m->Hkin > 0) {
+    g_cuda_err = "saturation hardening (sigsat > sigy0, delta > 0) with kinematic hardening (Hkin > 0) is not supported";
     return PFEM_ERR_BAD_ARG;
   }
   if (kind != PFEM_HEX8_SMALL && kind != PFEM_HEX8_FINITE && kind != PFEM_HEX8_FINITE_FBAR) {
@@ -1401,6 +1417,8 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
   ctx->nn = nn; ctx->ne = ne; ctx->ngp = 8 * ne; ctx->ndof = 3 * nn;
   ctx->kind = kind;
   ctx->mat.E = m->E; ctx->mat.nu = m->nu; ctx->mat.sigy0 = m->sigy0; ctx->mat.Hiso = m->Hiso; ctx->mat.Hkin = m->Hkin;
+  ctx->mat.sigsat = sigsat; ctx->mat.delta = m->delta; ctx->mat.sat = sigsat - m->sigy0;
+  ctx->hard = m->Hkin > 0 ? HARD_KIN : (voce ? HARD_VOCE : HARD_LINEAR);
   ctx->mat.G = m->E / (2.0 * (1.0 + m->nu));
   ctx->mat.K = m->E / (3.0 * (1.0 - 2.0 * m->nu));
   ctx->mat.lam = m->E * m->nu / ((1.0 + m->nu) * (1.0 - 2.0 * m->nu));
@@ -1512,6 +1530,7 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
   AL(ctx->dCpi, 6 * ctx->ngp);
   AL(ctx->dAlpha, ctx->ngp);
   AL(ctx->dEpsp, 6 * ctx->ngp);
+  if (ctx->hard == HARD_KIN) AL(ctx->dBeta, 6 * ctx->ngp);
   AL(ctx->dTau, 6 * ctx->ngp);
   AL(ctx->dFlags, ctx->ngp);
   AL(ctx->dU, ctx->ndof);
@@ -1707,7 +1726,8 @@ int pfem_reset(pfem_ctx* ctx) {
   if (!ctx) return PFEM_ERR_BAD_ARG;
   if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
   cudaSetDevice(ctx->device);
-  pfem::count_launch(); init_state_kernel<<<1024, 256, 0, ctx->st>>>(ctx->ngp, ctx->dCpi, ctx->dAlpha, ctx->dEpsp, ctx->dTau);
+  pfem::count_launch(); init_state_kernel<<<1024, 256, 0, ctx->st>>>(ctx->ngp, ctx->dCpi, ctx->dAlpha, ctx->dEpsp, ctx->dTau,
+                                                                     ctx->dBeta);
   CKL();
   CK(cudaMemsetAsync(ctx->dFlags, 0, ctx->ngp, ctx->st));
   CK(cudaMemsetAsync(ctx->dU, 0, ctx->ndof * sizeof(double), ctx->st));
@@ -1738,6 +1758,38 @@ int pfem_set_state(pfem_ctx* ctx, const double* cpi, const double* alpha, const 
   if (cpi && (rc = put(cpi, ctx->dCpi))) return rc;
   if (epsp && (rc = put(epsp, ctx->dEpsp))) return rc;
   if (alpha) CK(cudaMemcpy(ctx->dAlpha, alpha, ngp * sizeof(double), cudaMemcpyHostToDevice));
+  return PFEM_OK;
+}
+
+int pfem_get_back_stress(const pfem_ctx* ctx, double* beta) {
+  if (!ctx || !beta) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return PFEM_ERR_STATE;
+  const long long ngp = ctx->ngp;
+  if (!ctx->dBeta) {
+    std::fill(beta, beta + 6 * ngp, 0.0);
+    return PFEM_OK;
+  }
+  cudaSetDevice(ctx->device);
+  if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return PFEM_ERR_CUDA;
+  std::vector<double> t(6 * ngp);
+  if (cudaMemcpy(t.data(), ctx->dBeta, t.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return PFEM_ERR_CUDA;
+  for (long long g = 0; g < ngp; ++g)
+    for (int k = 0; k < 6; ++k) beta[g * 6 + k] = t[k * ngp + g];
+  return PFEM_OK;
+}
+
+int pfem_set_back_stress(pfem_ctx* ctx, const double* beta) {
+  if (!ctx || !beta) return PFEM_ERR_BAD_ARG;
+  if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
+  if (!ctx->dBeta) return fail(ctx, PFEM_ERR_BAD_ARG, "the model has no kinematic hardening (Hkin = 0)");
+  cudaSetDevice(ctx->device);
+  const long long ngp = ctx->ngp;
+  std::vector<double> t(6 * ngp);
+  for (long long g = 0; g < ngp; ++g)
+    for (int k = 0; k < 6; ++k) t[k * ngp + g] = beta[g * 6 + k];
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaMemcpy(ctx->dBeta, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
   return PFEM_OK;
 }
 

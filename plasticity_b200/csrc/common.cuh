@@ -29,8 +29,15 @@ inline void count_launch() { ++launch_counter(); }
 // (lagrangian/src/Materials.jl:104-107).
 struct MatParams {
   double E, nu, sigy0, Hiso, Hkin;
-  double G, K, lam;
+  double sigsat, delta;  // saturation hardening (Materials.jl:117-127); sat = sigsat - sigy0
+  double G, K, lam, sat;
 };
+
+// Hardening law of the element kernels (a template argument, fixed per model):
+// linear isotropic; saturation (Voce) isotropic, sigma_y(a) = sigy0 +
+// (sigsat - sigy0)(1 - exp(-delta a)) + Hiso a; linear kinematic (+ linear
+// isotropic), with the back stress as extra state.
+enum : int { HARD_LINEAR = 0, HARD_VOCE = 1, HARD_KIN = 2 };
 
 // Device status word.  code != 0 marks the first inverted Gauss point seen
 // (ElementInversionError, lagrangian/src/FiniteStrain.jl:42-52).

@@ -20,7 +20,8 @@
 //
 // Arithmetic follows the reference kernel element_force_tangent_finite!
 // (Elements.jl:405-494), finite_kinematics (FiniteStrain.jl:148-170),
-// return_map (Materials.jl:159-250, linear isotropic hardening, Hkin = 0),
+// return_map (Materials.jl:159-250; linear or saturation isotropic hardening,
+// or linear kinematic hardening through the polar rotation, HARD),
 // finite_stress_update (FiniteStrain.jl:292-346) and dPdF with
 // _dhalflog_contract (FiniteStrain.jl:463-547).  The return map is evaluated
 // on principal values: the trial stress is an isotropic function of b^e, so
@@ -58,12 +59,74 @@ __device__ __forceinline__ void dshape_a(int a, double x, double y, double z, do
   d[2] = 0.125 * za * (1.0 + xa * x) * (1.0 + ya * y);
 }
 
+// ---- saturation (Voce) hardening: yield_stress / yield_slope (Materials.jl:117-127)
+// and the scalar local Newton on dgamma of the plastic corrector (:201-213).
+// sy0 is the element's initial yield stress; m.sat = sigsat - sigy0.
+__device__ __forceinline__ double voce_ys(const MatParams& m, double sy0, double a) {
+  return sy0 + m.sat * (1.0 - exp(-m.delta * a)) + m.Hiso * a;
+}
+__device__ __forceinline__ double voce_slope(const MatParams& m, double a) {
+  return m.delta * m.sat * exp(-m.delta * a) + m.Hiso;
+}
+// Returns dgamma; *Hp receives the plastic modulus at alpha_n + dgamma.
+__device__ __forceinline__ double voce_dgamma(const MatParams& m, double sy0, double qtr, double an, double ftr,
+                                              double* Hp) {
+  const double c = 3.0 * m.G + m.Hkin;
+  double dg = ftr / (c + voce_slope(m, an));
+  for (int it = 0; it < 50; ++it) {
+    const double r = qtr - c * dg - voce_ys(m, sy0, an + dg);
+    const double d = r / (c + voce_slope(m, an + dg));
+    dg += d;
+    if (fabs(d) <= 1e-13 * (dg + 1e-14)) break;
+  }
+  *Hp = voce_slope(m, an + dg);
+  return dg;
+}
+
+// ---- symmetric 3x3 tensors packed as [00, 11, 22, 01, 12, 02] (physical shear) ----
+template <typename T>
+__device__ __forceinline__ void unpack_sym(const T* s, T* M) {
+  M[0] = s[0]; M[4] = s[1]; M[8] = s[2];
+  M[1] = s[3]; M[3] = s[3];
+  M[5] = s[4]; M[7] = s[4];
+  M[2] = s[5]; M[6] = s[5];
+}
+// out = A S A^T (S full symmetric), packed
+template <typename T>
+__device__ __forceinline__ void congruence(const T* A, const T* S, T* out) {
+  T AS[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) AS[3 * i + j] = A[3 * i] * S[j] + A[3 * i + 1] * S[3 + j] + A[3 * i + 2] * S[6 + j];
+  constexpr int I[6] = {0, 1, 2, 0, 1, 0}, J[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+    out[c] = AS[3 * I[c]] * A[3 * J[c]] + AS[3 * I[c] + 1] * A[3 * J[c] + 1] + AS[3 * I[c] + 2] * A[3 * J[c] + 2];
+}
+// out = A^T S A (S full symmetric), packed
+template <typename T>
+__device__ __forceinline__ void congruence_t(const T* A, const T* S, T* out) {
+  T At[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) At[3 * i + j] = A[3 * j + i];
+  congruence(At, S, out);
+}
+// Full contraction a : b of two packed symmetric tensors.
+template <typename T>
+__device__ __forceinline__ T sym_dot(const T* a, const T* b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + T(2) * (a[3] * b[3] + a[4] * b[4] + a[5] * b[5]);
+}
+
 // With FP32 tangent records the kernel is occupancy-bound: capping registers
 // for 11 resident one-warp blocks per SM (a little spilling to L1) measured
 // 14 % faster at 64^3 than the unconstrained 222 registers (9 blocks); the
 // FP64 variants lose from the same cap and keep the compiler's choice.
-template <typename KT, bool COMMIT, bool FBAR>
-__global__ void __launch_bounds__(32 * WPB, (std::is_same<KT, float>::value && !COMMIT) ? 11 : 1)
+// The kinematic variant carries more live state and keeps the compiler's choice.
+template <typename KT, bool COMMIT, bool FBAR, int HARD>
+__global__ void __launch_bounds__(32 * WPB, (std::is_same<KT, float>::value && !COMMIT && HARD != HARD_KIN) ? 11 : 1)
 element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   using TT = KT;  // type of the tangent records and of the phase-B arithmetic
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -227,31 +290,102 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   const double t0 = lam * tre + 2.0 * G * e0, t1 = lam * tre + 2.0 * G * e1, t2 = lam * tre + 2.0 * G * e2;
   const double pm = (t0 + t1 + t2) / 3.0;
   const double s0 = t0 - pm, s1 = t1 - pm, s2 = t2 - pm;
-  const double nrm = sqrt(s0 * s0 + s1 * s1 + s2 * s2);
   const double s32 = 1.22474487139158904910;  // sqrt(1.5)
+  // Kinematic hardening (finite_stress_update, FiniteStrain.jl:316-324): the
+  // back stress is stored in the reference configuration and pushed forward
+  // with the polar rotation of Fbar = R U (polar_RU, :194-210).  Everything
+  // below runs in b^e's eigenbasis Q: beta' = (Q^T R) beta_ref (Q^T R)^T, and
+  // the shifted stress xi' = diag(s) - beta' is no longer diagonal there, so
+  // the flow direction nh' is a full symmetric tensor.
+  double Rp[9], Vu[9], mu[3], QR[9], Bp[6], xi6[6], nh6[6];
+  double nrm;
+  if constexpr (HARD == HARD_KIN) {
+    double Cm[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Cm[3 * i + j] = Fb[i] * Fb[j] + Fb[3 + i] * Fb[3 + j] + Fb[6 + i] * Fb[6 + j];
+    double lc[3];
+    eig3_jacobi(Cm, lc, Vu);
+    double imu[3];
+#pragma unroll
+    for (int A = 0; A < 3; ++A) {
+      mu[A] = sqrt(fmax(lc[A], 0.0));
+      imu[A] = mu[A] > 0.0 ? 1.0 / mu[A] : 0.0;
+    }
+    double Ui[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Ui[3 * i + j] = Vu[3 * i] * imu[0] * Vu[3 * j] + Vu[3 * i + 1] * imu[1] * Vu[3 * j + 1] + Vu[3 * i + 2] * imu[2] * Vu[3 * j + 2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Rp[3 * i + j] = Fb[3 * i] * Ui[j] + Fb[3 * i + 1] * Ui[3 + j] + Fb[3 * i + 2] * Ui[6 + j];
+#pragma unroll
+    for (int A = 0; A < 3; ++A)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) QR[3 * A + k] = Q[A] * Rp[k] + Q[3 + A] * Rp[3 + k] + Q[6 + A] * Rp[6 + k];
+    double b6[6], Bf[9];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) b6[c] = p.beta[(long long)c * p.ngp + gp];
+    unpack_sym(b6, Bf);
+    congruence(QR, Bf, Bp);
+    xi6[0] = s0 - Bp[0]; xi6[1] = s1 - Bp[1]; xi6[2] = s2 - Bp[2];
+    xi6[3] = -Bp[3]; xi6[4] = -Bp[4]; xi6[5] = -Bp[5];
+    nrm = sqrt(sym_dot(xi6, xi6));
+  } else {
+    nrm = sqrt(s0 * s0 + s1 * s1 + s2 * s2);
+  }
   const double qtr = s32 * nrm;
-  const double ftr = qtr - (sy0 + H * an);
+  const double ftr = (HARD == HARD_VOCE) ? qtr - voce_ys(m, sy0, an) : qtr - (sy0 + H * an);
   const bool plastic = ftr > 0.0;
   double n0 = 0.0, n1 = 0.0, n2 = 0.0, dg = 0.0, b0 = 0.0, g0c = 0.0;
   double ta0 = t0, ta1 = t1, ta2 = t2;
   if (plastic) {
-    n0 = s0 / nrm; n1 = s1 / nrm; n2 = s2 / nrm;
-    dg = ftr / (3.0 * G + H);
-    const double c = 2.0 * G * dg * s32;
-    ta0 = t0 - c * n0; ta1 = t1 - c * n1; ta2 = t2 - c * n2;
-    b0 = 2.0 * G * dg / qtr;
-    g0c = 2.0 * G / (3.0 * G + H);
-  }
-  // tau = Q diag(tau_A) Q^T  (Kirchhoff, physical-shear Voigt)
-  double tau[9];
+    if constexpr (HARD == HARD_KIN) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = i; j < 3; ++j) {
-      const double v = Q[3 * i] * ta0 * Q[3 * j] + Q[3 * i + 1] * ta1 * Q[3 * j + 1] + Q[3 * i + 2] * ta2 * Q[3 * j + 2];
-      tau[3 * i + j] = v;
-      tau[3 * j + i] = v;
+      for (int c = 0; c < 6; ++c) nh6[c] = xi6[c] / nrm;
+      dg = ftr / (3.0 * G + H + m.Hkin);
+      g0c = 2.0 * G / (3.0 * G + m.Hkin + H);
+    } else {
+      n0 = s0 / nrm; n1 = s1 / nrm; n2 = s2 / nrm;
+      if constexpr (HARD == HARD_VOCE) {
+        double Hp;
+        dg = voce_dgamma(m, sy0, qtr, an, ftr, &Hp);
+        g0c = 2.0 * G / (3.0 * G + Hp);
+      } else {
+        dg = ftr / (3.0 * G + H);
+        g0c = 2.0 * G / (3.0 * G + H);
+      }
+      const double c = 2.0 * G * dg * s32;
+      ta0 = t0 - c * n0; ta1 = t1 - c * n1; ta2 = t2 - c * n2;
     }
+    b0 = 2.0 * G * dg / qtr;
+  } else if constexpr (HARD == HARD_KIN) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) nh6[c] = 0.0;
+  }
+  // tau = Q tau' Q^T  (Kirchhoff, physical-shear Voigt); tau' is diagonal
+  // unless kinematic hardening tilts the flow direction.
+  double tau[9];
+  if constexpr (HARD == HARD_KIN) {
+    const double c = 2.0 * G * dg * s32;
+    const double tp[6] = {t0 - c * nh6[0], t1 - c * nh6[1], t2 - c * nh6[2], -c * nh6[3], -c * nh6[4], -c * nh6[5]};
+    double Tf[9], t6[6];
+    unpack_sym(tp, Tf);
+    congruence(Q, Tf, t6);
+    unpack_sym(t6, tau);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = i; j < 3; ++j) {
+        const double v = Q[3 * i] * ta0 * Q[3 * j] + Q[3 * i + 1] * ta1 * Q[3 * j + 1] + Q[3 * i + 2] * ta2 * Q[3 * j + 2];
+        tau[3 * i + j] = v;
+        tau[3 * j + i] = v;
+      }
+  }
   if (valid) {
     p.tau[0 * p.ngp + gp] = tau[0];
     p.tau[1 * p.ngp + gp] = tau[4];
@@ -263,7 +397,52 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   }
   double Fbi[9];
   inv3(Fb, Fbi);
-  if constexpr (COMMIT) {
+  if constexpr (COMMIT && HARD == HARD_KIN) {
+    if (!valid) return;
+    const double c = dg * s32;
+    // back stress: beta_sp' + (2/3) Hkin dgamma sqrt(3/2) nh', pulled back to the
+    // reference configuration, beta_ref = R^T beta_sp R (FiniteStrain.jl:324)
+    double bn[6], Bf[9], b6n[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) bn[k] = Bp[k] + (2.0 / 3.0) * m.Hkin * c * nh6[k];
+    unpack_sym(bn, Bf);
+    congruence_t(QR, Bf, b6n);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) p.beta[(long long)k * p.ngp + gp] = b6n[k];
+    // exponential map with a flow direction that is not coaxial with b^e:
+    // b^e_{n+1} = exp(2 eps^e'), eps^e' = diag(e) - dgamma sqrt(3/2) nh'
+    // (FiniteStrain.jl:331-343), Cp^-1 = Fbar^-1 Q b^e' Q^T Fbar^-T.
+    const double ee[6] = {2.0 * (e0 - c * nh6[0]), 2.0 * (e1 - c * nh6[1]), 2.0 * (e2 - c * nh6[2]),
+                          -2.0 * c * nh6[3], -2.0 * c * nh6[4], -2.0 * c * nh6[5]};
+    double E2[9], w2[3], V2[9];
+    unpack_sym(ee, E2);
+    eig3_jacobi(E2, w2, V2);
+    double FQ[9], T[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int A = 0; A < 3; ++A) FQ[3 * i + A] = Fbi[3 * i] * Q[A] + Fbi[3 * i + 1] * Q[3 + A] + Fbi[3 * i + 2] * Q[6 + A];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int A = 0; A < 3; ++A) T[3 * i + A] = FQ[3 * i] * V2[A] + FQ[3 * i + 1] * V2[3 + A] + FQ[3 * i + 2] * V2[6 + A];
+    const double l0 = exp(w2[0]), l1 = exp(w2[1]), l2 = exp(w2[2]);
+    constexpr int I6[6] = {0, 1, 2, 0, 1, 0}, J6[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const int i = I6[k], j = J6[k];
+      p.cpi[(long long)k * p.ngp + gp] = T[3 * i] * l0 * T[3 * j] + T[3 * i + 1] * l1 * T[3 * j + 1] + T[3 * i + 2] * l2 * T[3 * j + 2];
+    }
+    p.alpha[gp] = an + dg;
+    // accumulated plastic strain Q (c nh') Q^T (diagnostic; engineering-shear Voigt)
+    double cn6[6], Nf[9], d6[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cn6[k] = c * nh6[k];
+    unpack_sym(cn6, Nf);
+    congruence(Q, Nf, d6);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) p.epsp[(long long)k * p.ngp + gp] += (k < 3 ? 1.0 : 2.0) * d6[k];
+  } else if constexpr (COMMIT) {
     if (!valid) return;
     // exponential-map update b^e_{n+1} = exp(2 eps^e), Cp^-1 = F^-1 b^e F^-T
     // (FiniteStrain.jl:331-343); eps^e shares the trial eigenbasis.
@@ -378,6 +557,36 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
     const TT c1 = (TT)(lam + G * b0);
     const TT c3 = (TT)(3.0 * G * (b0 - g0c));
     const TT nv[3] = {(TT)n0, (TT)n1, (TT)n2};
+    // Kinematic hardening: the flow direction nh' (full in the eigenbasis) and
+    // the back-stress rotation coupling dtau/dbeta_sp . dbeta_sp/dFbar of dPdF
+    // (FiniteStrain.jl:532-536) with dtau/dbeta = a I + kd xi (x) xi
+    // (dtau_dbeta, :250-268; zero in the elastic branch).  Per column the polar
+    // spin follows from Omega U + U Omega = R^T dF - dF^T R in U's eigenbasis V
+    // (dR_polar, :220-233): dbeta' = W' beta' + (W' beta')^T, W' = M Ob M^T,
+    // M = Q^T R V.
+    TT nhk[6], xik[6], Bk[9], M3[9], RV[9], Vk[9], muk[3], ask = TT(0), kdk = TT(0);
+    if constexpr (HARD == HARD_KIN) {
+      double Bf[9];
+      unpack_sym(Bp, Bf);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) { nhk[k] = (TT)nh6[k]; xik[k] = (TT)xi6[k]; }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          Bk[3 * i + j] = (TT)Bf[3 * i + j];
+          Vk[3 * i + j] = (TT)Vu[3 * i + j];
+          M3[3 * i + j] = (TT)(QR[3 * i] * Vu[j] + QR[3 * i + 1] * Vu[3 + j] + QR[3 * i + 2] * Vu[6 + j]);
+          RV[3 * i + j] = (TT)(Rp[3 * i] * Vu[j] + Rp[3 * i + 1] * Vu[3 + j] + Rp[3 * i + 2] * Vu[6 + j]);
+        }
+#pragma unroll
+      for (int A = 0; A < 3; ++A) muk[A] = (TT)mu[A];
+      if (plastic) {
+        const double Yy = sy0 + H * an;
+        ask = (TT)(2.0 * G * s32 * dg / nrm);
+        kdk = (TT)(2.0 * G * s32 / (3.0 * G + H + m.Hkin) * (Yy / (nrm * nrm)) / nrm);
+      }
+    }
     const TT ws_ = (TT)(w * scale);
     TT* const As = Rg + 24;  // [(j*3+i)*9 + (q*3+p)]
     TT uacc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -395,13 +604,51 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
           Y[3 * B + A] = v;
         }
       const TT trY = Y[0] + Y[4] + Y[8];
-      const TT nd = nv[0] * Y[0] + nv[1] * Y[4] + nv[2] * Y[8];
       TT dt[9];
 #pragma unroll
       for (int i = 0; i < 9; ++i) dt[i] = c2 * Y[i];
-      dt[0] += c1 * trY + c3 * nd * nv[0];
-      dt[4] += c1 * trY + c3 * nd * nv[1];
-      dt[8] += c1 * trY + c3 * nd * nv[2];
+      if constexpr (HARD == HARD_KIN) {
+        const TT Ys[6] = {Y[0], Y[4], Y[8], Y[1], Y[5], Y[2]};
+        const TT nd = sym_dot(nhk, Ys);
+        TT add[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) add[k] = c3 * nd * nhk[k];
+        add[0] += c1 * trY; add[1] += c1 * trY; add[2] += c1 * trY;
+        if (ask != TT(0)) {
+          const TT* av = RV + 3 * pp;  // row pp of R V
+          const TT* cv = Vk + 3 * qq;  // row qq of V
+          const TT w01 = (av[0] * cv[1] - cv[0] * av[1]) / (muk[0] + muk[1]);
+          const TT w02 = (av[0] * cv[2] - cv[0] * av[2]) / (muk[0] + muk[2]);
+          const TT w12 = (av[1] * cv[2] - cv[1] * av[2]) / (muk[1] + muk[2]);
+          const TT Ob[9] = {TT(0), w01, w02, -w01, TT(0), w12, -w02, -w12, TT(0)};
+          TT MO[9], Wp[9], X[9];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) MO[3 * i + j] = M3[3 * i] * Ob[j] + M3[3 * i + 1] * Ob[3 + j] + M3[3 * i + 2] * Ob[6 + j];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) Wp[3 * i + j] = MO[3 * i] * M3[3 * j] + MO[3 * i + 1] * M3[3 * j + 1] + MO[3 * i + 2] * M3[3 * j + 2];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) X[3 * i + j] = Wp[3 * i] * Bk[j] + Wp[3 * i + 1] * Bk[3 + j] + Wp[3 * i + 2] * Bk[6 + j];
+          const TT db[6] = {TT(2) * X[0], TT(2) * X[4], TT(2) * X[8], X[1] + X[3], X[5] + X[7], X[2] + X[6]};
+          const TT xd = kdk * sym_dot(xik, db);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) add[k] += ask * db[k] + xd * xik[k];
+        }
+        dt[0] += add[0]; dt[4] += add[1]; dt[8] += add[2];
+        dt[1] += add[3]; dt[3] += add[3];
+        dt[5] += add[4]; dt[7] += add[4];
+        dt[2] += add[5]; dt[6] += add[5];
+      } else {
+        const TT nd = nv[0] * Y[0] + nv[1] * Y[4] + nv[2] * Y[8];
+        dt[0] += c1 * trY + c3 * nd * nv[0];
+        dt[4] += c1 * trY + c3 * nd * nv[1];
+        dt[8] += c1 * trY + c3 * nd * nv[2];
+      }
       TT T[9];  // dt' N
 #pragma unroll
       for (int A = 0; A < 3; ++A)
@@ -473,7 +720,7 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   }  // !COMMIT
 }
 
-template <typename KT, bool COMMIT, bool FBAR>
+template <typename KT, bool COMMIT, bool FBAR, int HARD>
 static void launch_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_t st) {
   if (n <= 0) return;
   const int warps = (n + EPW - 1) / EPW;
@@ -481,17 +728,18 @@ static void launch_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_
   const size_t sm = (size_t)WPB * warp_smem_bytes<KT>(COMMIT);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(element_color_kernel<KT, COMMIT, FBAR>,
+    cudaFuncSetAttribute(element_color_kernel<KT, COMMIT, FBAR, HARD>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     attr = true;
   }
-  pfem::count_launch(); element_color_kernel<KT, COMMIT, FBAR><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
+  pfem::count_launch(); element_color_kernel<KT, COMMIT, FBAR, HARD><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
 }
 
 // ---------------------------------------------------------------- small strain
 // The small-strain kind, element_force_tangent! (Elements.jl:323-360) with
-// bmatrix (:97-117) and the Voigt return map (Materials.jl:159-250, linear
-// isotropic hardening, Hkin = 0 so the back stress stays zero).  Same warp
+// bmatrix (:97-117) and the Voigt return map (Materials.jl:159-250; linear or
+// saturation isotropic hardening, or linear kinematic hardening with the back
+// stress in p.beta, HARD).  Same warp
 // organisation as the finite kernel: a lane evaluates one Gauss point
 // (strain, return map, stress, consistent tangent D in FP64), the forces are
 // shuffle-reduced node by node, the records (dN/dX, w D) go to shared memory in
@@ -506,7 +754,7 @@ constexpr int warp_smem_small(bool commit) {
 }
 static_assert(8 * SREC * 4 >= 48 * 8, "coordinate scratch must fit in the record area");
 
-template <typename KT, bool COMMIT>
+template <typename KT, bool COMMIT, int HARD>
 __global__ void __launch_bounds__(32 * WPB)
 element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   using TT = KT;
@@ -569,7 +817,7 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
     eps[5] += nz * ux + nx * uz;
   }
   __syncwarp();  // the nodal coordinates are dead; the records may overwrite them
-  // ---- return_map, Materials.jl:159-250 (Hkin = 0, beta = 0) ----
+  // ---- return_map, Materials.jl:159-250 ----
   const double G = m.G, lam = m.lam, H = m.Hiso;
   const double sy0 = p.sigy0_e ? p.sigy0_e[e] : m.sigy0;
   const double an = p.alpha[gp];
@@ -583,22 +831,34 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
 #pragma unroll
   for (int c = 3; c < 6; ++c) st[c] = G * de[c];
   const double pm = (st[0] + st[1] + st[2]) / 3.0;
-  double xi[6];
+  double xi[6], bn[6];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) xi[c] = st[c] - (c < 3 ? pm : 0.0);
+  for (int c = 0; c < 6; ++c) {
+    bn[c] = (HARD == HARD_KIN) ? p.beta[(long long)c * p.ngp + gp] : 0.0;
+    xi[c] = st[c] - (c < 3 ? pm : 0.0) - bn[c];
+  }
   const double nrm = sqrt(xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2] +
                           2.0 * (xi[3] * xi[3] + xi[4] * xi[4] + xi[5] * xi[5]));
   const double s32 = 1.22474487139158904910;
   const double qtr = s32 * nrm;
-  const double ftr = qtr - (sy0 + H * an);
+  const double ftr = (HARD == HARD_VOCE) ? qtr - voce_ys(m, sy0, an) : qtr - (sy0 + H * an);
   const bool plastic = ftr > 0.0;
   double nh[6] = {0, 0, 0, 0, 0, 0}, sig[6], dg = 0.0, b0 = 0.0, g0c = 0.0;
   if (plastic) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) nh[c] = xi[c] / nrm;
-    dg = ftr / (3.0 * G + H);
+    if constexpr (HARD == HARD_VOCE) {
+      double Hp;
+      dg = voce_dgamma(m, sy0, qtr, an, ftr, &Hp);
+      g0c = 2.0 * G / (3.0 * G + Hp);
+    } else if constexpr (HARD == HARD_KIN) {
+      dg = ftr / (3.0 * G + H + m.Hkin);
+      g0c = 2.0 * G / (3.0 * G + m.Hkin + H);
+    } else {
+      dg = ftr / (3.0 * G + H);
+      g0c = 2.0 * G / (3.0 * G + H);
+    }
     b0 = 2.0 * G * dg / qtr;
-    g0c = 2.0 * G / (3.0 * G + H);
   }
 #pragma unroll
   for (int c = 0; c < 6; ++c) sig[c] = st[c] - (2.0 * G * dg * s32) * nh[c];
@@ -612,6 +872,10 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
 #pragma unroll
     for (int c = 0; c < 6; ++c)
       p.epsp[(long long)c * p.ngp + gp] += (dg * s32) * (c < 3 ? nh[c] : 2.0 * nh[c]);
+    if constexpr (HARD == HARD_KIN) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) p.beta[(long long)c * p.ngp + gp] = bn[c] + (2.0 / 3.0) * m.Hkin * (dg * s32) * nh[c];
+    }
     p.alpha[gp] = an + dg;
   } else {
     // ---- internal force, node by node (FP64), lane g keeps node g ----
@@ -709,7 +973,7 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
   }
 }
 
-template <typename KT, bool COMMIT>
+template <typename KT, bool COMMIT, int HARD>
 static void launch_small_t(const ElemArgs<KT>& a, const int* elist, int n, cudaStream_t st) {
   if (n <= 0) return;
   const int warps = (n + EPW - 1) / EPW;
@@ -717,34 +981,48 @@ static void launch_small_t(const ElemArgs<KT>& a, const int* elist, int n, cudaS
   const size_t sm = (size_t)WPB * warp_smem_small<KT>(COMMIT);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(element_small_kernel<KT, COMMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(element_small_kernel<KT, COMMIT, HARD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     attr = true;
   }
   pfem::count_launch();
-  element_small_kernel<KT, COMMIT><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
+  element_small_kernel<KT, COMMIT, HARD><<<blocks, 32 * WPB, sm, st>>>(a, elist, n);
+}
+
+template <typename KT, int HARD>
+static void launch_small_h(const ElemArgs<KT>& a, const int* elist, int n, bool commit, cudaStream_t st) {
+  if (commit) launch_small_t<KT, true, HARD>(a, elist, n, st);
+  else launch_small_t<KT, false, HARD>(a, elist, n, st);
 }
 
 template <typename KT>
-void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, cudaStream_t st) {
-  if (commit) launch_small_t<KT, true>(a, elist, n, st);
-  else launch_small_t<KT, false>(a, elist, n, st);
+void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, int hard, cudaStream_t st) {
+  if (hard == HARD_KIN) launch_small_h<KT, HARD_KIN>(a, elist, n, commit, st);
+  else if (hard == HARD_VOCE) launch_small_h<KT, HARD_VOCE>(a, elist, n, commit, st);
+  else launch_small_h<KT, HARD_LINEAR>(a, elist, n, commit, st);
 }
-template void launch_element_small<double>(const ElemArgs<double>&, const int*, int, bool, cudaStream_t);
-template void launch_element_small<float>(const ElemArgs<float>&, const int*, int, bool, cudaStream_t);
+template void launch_element_small<double>(const ElemArgs<double>&, const int*, int, bool, int, cudaStream_t);
+template void launch_element_small<float>(const ElemArgs<float>&, const int*, int, bool, int, cudaStream_t);
 
-template <typename KT>
-void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit,
-                          bool fbar, cudaStream_t st) {
+template <typename KT, int HARD>
+static void launch_color_h(const ElemArgs<KT>& a, const int* elist, int n, bool commit, bool fbar, cudaStream_t st) {
   if (commit) {
-    if (fbar) launch_t<KT, true, true>(a, elist, n, st);
-    else launch_t<KT, true, false>(a, elist, n, st);
+    if (fbar) launch_t<KT, true, true, HARD>(a, elist, n, st);
+    else launch_t<KT, true, false, HARD>(a, elist, n, st);
   } else {
-    if (fbar) launch_t<KT, false, true>(a, elist, n, st);
-    else launch_t<KT, false, false>(a, elist, n, st);
+    if (fbar) launch_t<KT, false, true, HARD>(a, elist, n, st);
+    else launch_t<KT, false, false, HARD>(a, elist, n, st);
   }
 }
 
-template void launch_element_color<double>(const ElemArgs<double>&, const int*, int, bool, bool, cudaStream_t);
-template void launch_element_color<float>(const ElemArgs<float>&, const int*, int, bool, bool, cudaStream_t);
+template <typename KT>
+void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit,
+                          bool fbar, int hard, cudaStream_t st) {
+  if (hard == HARD_KIN) launch_color_h<KT, HARD_KIN>(a, elist, n, commit, fbar, st);
+  else if (hard == HARD_VOCE) launch_color_h<KT, HARD_VOCE>(a, elist, n, commit, fbar, st);
+  else launch_color_h<KT, HARD_LINEAR>(a, elist, n, commit, fbar, st);
+}
+
+template void launch_element_color<double>(const ElemArgs<double>&, const int*, int, bool, bool, int, cudaStream_t);
+template void launch_element_color<float>(const ElemArgs<float>&, const int*, int, bool, bool, int, cudaStream_t);
 
 }  // namespace pfem

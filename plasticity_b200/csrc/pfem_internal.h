@@ -17,6 +17,8 @@ struct ElemArgs {
   double* cpi;             // 6 x ngp committed Cp^-1 (component-major SoA)
   double* alpha;           // ngp committed equivalent plastic strain
   double* epsp;            // 6 x ngp accumulated plastic strain (diagnostic)
+  double* beta;            // 6 x ngp committed back stress (HARD_KIN only; reference
+                           // configuration for the finite kinds), else null
   const double* sigy0_e;   // ne per-element initial yield stress, or null
   double* tau;             // 6 x ngp Kirchhoff stress of the last evaluation
   uint8_t* flags;          // ngp elastic(0)/plastic(1) of the last evaluation
@@ -31,11 +33,12 @@ struct ElemArgs {
 
 template <typename KT>
 void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool commit, bool fbar,
-                          cudaStream_t st);
+                          int hard, cudaStream_t st);
 // Small-strain kind (Elements.jl:323-360): epsp holds the committed plastic
 // strain, tau receives sigma; cpi is unused.
 template <typename KT>
-void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, cudaStream_t st);
+void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, int hard,
+                          cudaStream_t st);
 
 // ---------------- block-CSR matrices ----------------
 template <typename VT>

@@ -84,12 +84,16 @@ def dof(node, comp):
 # ------------------------------------------------------------------ material
 @dataclass
 class J2Material:
-    """J2Material (Materials.jl:68-108), linear isotropic hardening (Hkin = 0 on this path)."""
+    """J2Material (Materials.jl:68-108): isotropic hardening
+    sigma_y(a) = sigy0 + (sigsat - sigy0)(1 - exp(-delta a)) + Hiso a (yield_stress,
+    :117-118; linear when delta = 0 or sigsat = sigy0) and linear kinematic hardening Hkin."""
     E: float
     nu: float
     sigy0: float
     Hiso: float = 0.0
     Hkin: float = 0.0
+    sigsat: float | None = None   # keyword default: sigy0
+    delta: float = 0.0
 
     def __post_init__(self):
         # ArgumentError guards, Materials.jl:90-103
@@ -101,6 +105,19 @@ class J2Material:
             raise ValueError(f"sigy0 must be positive (got {self.sigy0})")
         if self.Hiso < 0 or self.Hkin < 0:
             raise ValueError("hardening moduli must be >= 0")
+        if self.sigsat is None:
+            self.sigsat = self.sigy0
+        if not self.sigsat >= self.sigy0:
+            raise ValueError(f"sigsat must be >= sigy0 (got sigsat={self.sigsat}, sigy0={self.sigy0})")
+        if not self.delta >= 0:
+            raise ValueError(f"delta must be >= 0 (got {self.delta})")
+        if self.delta > 0 and self.sigsat > self.sigy0 and self.Hkin > 0:
+            raise ValueError("saturation hardening (sigsat>sigy0, delta>0) with kinematic hardening "
+                             "(Hkin>0) is not supported; use one or the other")
+
+    def yield_stress(self, a):
+        """yield_stress (Materials.jl:117-118)."""
+        return self.sigy0 + (self.sigsat - self.sigy0) * (1 - np.exp(-self.delta * a)) + self.Hiso * a
 
     @property
     def G(self):
@@ -111,7 +128,7 @@ class J2Material:
         return self.E * self.nu / ((1 + self.nu) * (1 - 2 * self.nu))
 
     def _c(self) -> L.Material:
-        return L.Material(self.E, self.nu, self.sigy0, self.Hiso, self.Hkin)
+        return L.Material(self.E, self.nu, self.sigy0, self.Hiso, self.Hkin, self.sigsat, self.delta)
 
 
 @dataclass
@@ -259,7 +276,8 @@ class Model:
 
     def _opts(self, nsteps=10, tol=1e-8, maxiter=25, precision="fp64", linsolve="cg", lin_rtol=None,
               predictor="previous", amg_rebuild=False, cheb_degree=2, cg_itmax=200, eta_min=None,
-              line_search=False, verbose=False, predictor_smooth=None, eta_max=None, max_cuts=0):
+              line_search=False, verbose=False, predictor_smooth=None, eta_max=None, max_cuts=0,
+              eta_first=None):
         o = L.SolveOpts()
         L.lib().pfem_default_opts(C.byref(o))
         o.nsteps, o.maxiter, o.tol = nsteps, maxiter, tol
@@ -281,6 +299,8 @@ class Model:
         if eta_max is not None:
             o.eta_max = float(eta_max)
         o.max_cuts = int(max_cuts)
+        if eta_first is not None:
+            o.eta_first = float(eta_first)
         return o
 
     def solve(self, nsteps=10, tol=1e-8, maxiter=25, **kw) -> SolveResult:
@@ -369,6 +389,18 @@ class Model:
         a = None if alpha is None else np.ascontiguousarray(alpha, np.float64)
         e = None if epsp is None else np.ascontiguousarray(epsp, np.float64)
         check(L.lib().pfem_set_state(self._ctx, ptr(c), ptr(a), ptr(e)), self._ctx)
+
+    def back_stress(self):
+        """Committed back stress (GaussState.beta, Mesh.jl:124-130), shape (ngp, 6);
+        the rotation-neutralised (reference-configuration) back stress for the
+        finite kinds, zeros when Hkin = 0."""
+        b = np.zeros((self.ngp, 6))
+        check(L.lib().pfem_get_back_stress(self._ctx, ptr(b)), self._ctx)
+        return b
+
+    def set_back_stress(self, beta):
+        b = np.ascontiguousarray(beta, np.float64)
+        check(L.lib().pfem_set_back_stress(self._ctx, ptr(b)), self._ctx)
 
     def set_displacement(self, U):
         U = np.ascontiguousarray(U, np.float64)

@@ -32,10 +32,26 @@ def test_library_exports_every_header_symbol():
 def test_bad_arguments_rejected():
     lib = L.lib()
     ctx = C.c_void_p()
-    m = L.Material(210e3, 0.3, 250.0, 1000.0, 500.0)       # Hkin > 0 is out of this path
     nodes = np.zeros((8, 3)); el = np.arange(1, 9, dtype=np.int64).reshape(1, 8)
-    rc = lib.pfem_create(C.byref(ctx), L.ptr(nodes), 8, L.ptr(el, L._i64), 1, 2, C.byref(m), None, -1)
-    assert rc == L.PFEM_ERR_BAD_ARG
+    # test_saturation.jl:128-140 (T15): saturation with Hkin > 0, sigsat < sigy0, delta < 0
+    for m in (L.Material(206.9e3, 0.29, 450.0, 129.24, 100.0, 715.0, 16.93),
+              L.Material(210e3, 0.3, 450.0, 0.0, 0.0, 400.0, 10.0),
+              L.Material(210e3, 0.3, 450.0, 0.0, 0.0, 715.0, -1.0)):
+        rc = lib.pfem_create(C.byref(ctx), L.ptr(nodes), 8, L.ptr(el, L._i64), 1, 2, C.byref(m), None, -1)
+        assert rc == L.PFEM_ERR_BAD_ARG
+    for kw in (dict(sigsat=715.0, delta=16.93, Hiso=129.24, Hkin=100.0), dict(sigsat=400.0, delta=10.0),
+               dict(sigsat=715.0, delta=-1.0)):
+        with pytest.raises(ValueError):
+            P.J2Material(210e3, 0.3, 450.0, **kw)
+    mlin = P.J2Material(210e3, 0.3, 250.0, Hiso=1000.0)
+    assert mlin.sigsat == mlin.sigy0 and mlin.delta == 0.0
+    # kinematic and saturation materials are accepted (topology-only context)
+    for m in (L.Material(210e3, 0.3, 250.0, 200.0, 2000.0, 0.0, 0.0),
+              L.Material(206.9e3, 0.29, 450.0, 129.24, 0.0, 715.0, 16.93)):
+        c2 = C.c_void_p()
+        rc = lib.pfem_create(C.byref(c2), L.ptr(nodes), 8, L.ptr(el, L._i64), 1, 2, C.byref(m), None, -1)
+        assert rc == 0
+        lib.pfem_destroy(c2)
     m = L.Material(210e3, 0.6, 250.0, 0.0, 0.0)            # nu >= 0.5 (Materials.jl:91)
     rc = lib.pfem_create(C.byref(ctx), L.ptr(nodes), 8, L.ptr(el, L._i64), 1, 2, C.byref(m), None, -1)
     assert rc == L.PFEM_ERR_BAD_ARG
