@@ -202,18 +202,100 @@ void par_for(long long n, Fn fn) {
   for (auto& t : th) t.join();
 }
 
+// par_for over contiguous chunks: fn(begin, end) once per thread, so a thread
+// can keep scratch (marker arrays) across its rows.
+template <typename Fn>
+void par_chunks(long long n, Fn fn) {
+  const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 20000 || nt == 1) {
+    fn(0ll, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long long chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    const long long b = t * chunk, e = std::min(n, b + chunk);
+    if (b >= e) break;
+    th.emplace_back([=, &fn]() { fn(b, e); });
+  }
+  for (auto& t : th) t.join();
+}
+
+// Symbolic sparse product (Gustavson): row r of the result is the sorted set
+// of map(j) over j in B(k), k in A(r), with A = (arp, acl) and B = (brp, bcl);
+// brp = null means B(k) = {k}; map = null is the identity.  Columns lie in
+// [0, ncols).  Two passes with a per-thread marker array: counts, then fill
+// and sort each (short) row.
+void symbolic_product(int nrows, const int* arp, const int* acl, const int* brp, const int* bcl,
+                      const int* map, int ncols, std::vector<int>& rp, std::vector<int>& cl) {
+  rp.assign((size_t)nrows + 1, 0);
+  auto visit = [&](int r, std::vector<int>& mark, auto&& emit) {
+    for (int t = arp[r]; t < arp[r + 1]; ++t) {
+      const int k = acl[t];
+      const int q0 = brp ? brp[k] : 0, q1 = brp ? brp[k + 1] : 1;
+      for (int q = q0; q < q1; ++q) {
+        const int j0 = brp ? bcl[q] : k;
+        const int j = map ? map[j0] : j0;
+        if (mark[j] != r) { mark[j] = r; emit(j); }
+      }
+    }
+  };
+  par_chunks(nrows, [&](long long b, long long e) {
+    std::vector<int> mark(ncols, -1);
+    for (long long r = b; r < e; ++r) {
+      int cnt = 0;
+      visit((int)r, mark, [&](int) { ++cnt; });
+      rp[r + 1] = cnt;
+    }
+  });
+  for (int r = 0; r < nrows; ++r) rp[r + 1] += rp[r];
+  cl.resize(rp[nrows]);
+  par_chunks(nrows, [&](long long b, long long e) {
+    std::vector<int> mark(ncols, -1);
+    for (long long r = b; r < e; ++r) {
+      int* o = cl.data() + rp[r];
+      int n = 0;
+      visit((int)r, mark, [&](int j) { o[n++] = j; });
+      std::sort(o, o + n);
+    }
+  });
+}
+
 // element_colors reference rule (Assembly.jl:172-206): parity colors when
 // the node coordinates form an axis-aligned structured box, else one color.
 int reference_colors(const std::vector<double>& X, long long nn, long long ne,
                      std::vector<int64_t>& color) {
   color.assign(ne, 0);
   if (ne == 0) return 0;
+  // _box_dims: distinct rounded coordinates per axis.  A box needs at least
+  // two distinct values on each of the other axes, so more than nn/4 on one
+  // axis already rules it out and the count stops there.
   long long dims[3];
+  const long long cap = nn / 4;
+  size_t tsize = 16;
+  while (tsize < (size_t)(2 * cap + 2)) tsize <<= 1;
+  std::vector<uint64_t> table(tsize);
+  std::vector<uint8_t> used(tsize);
   for (int d = 0; d < 3; ++d) {
-    std::vector<double> v(nn);
-    for (long long n = 0; n < nn; ++n) v[n] = std::round(X[n * 3 + d] * 1e12) / 1e12;
-    std::sort(v.begin(), v.end());
-    dims[d] = (long long)(std::unique(v.begin(), v.end()) - v.begin()) - 1;
+    // open-addressing set of the rounded values' bit patterns (-0.0 folded
+    // into 0.0, so membership is numeric equality)
+    std::fill(used.begin(), used.end(), 0);
+    long long count = 0;
+    for (long long n = 0; n < nn && count <= cap; ++n) {
+      double v = std::round(X[n * 3 + d] * 1e12) / 1e12;
+      if (v == 0.0) v = 0.0;
+      uint64_t key;
+      std::memcpy(&key, &v, sizeof(key));
+      size_t h = (size_t)((key * 0x9E3779B97F4A7C15ull) >> 17) & (tsize - 1);
+      while (used[h] && table[h] != key) h = (h + 1) & (tsize - 1);
+      if (!used[h]) {
+        used[h] = 1;
+        table[h] = key;
+        ++count;
+      }
+    }
+    if (count > cap) return 1;
+    dims[d] = count - 1;
   }
   const long long nx = dims[0], ny = dims[1], nz = dims[2];
   if (!(nx >= 1 && ny >= 1 && nz >= 1 && nx * ny * nz == ne && (nx + 1) * (ny + 1) * (nz + 1) == nn))
@@ -267,7 +349,7 @@ int greedy_colors(const std::vector<int>& elem, long long nn, long long ne, std:
 // Greedy aggregation on a block graph: phase 1 roots whose neighbourhood is
 // untouched, phase 2 attaches leftovers to an adjacent aggregate, phase 3
 // groups whatever remains with its unaggregated neighbours.
-int aggregate(int nb, const std::vector<int>& rp, const std::vector<int>& cl, std::vector<int>& agg) {
+int aggregate(int nb, const int* rp, const int* cl, std::vector<int>& agg) {
   agg.assign(nb, -1);
   int na = 0;
   for (int n = 0; n < nb; ++n) {
@@ -326,25 +408,16 @@ void mgs_qr(int m, std::vector<double>& A, double R[36]) {
   }
 }
 
-// Sorted union of the column lists of a set of rows.
-void sorted_union(std::vector<int>& out) {
-  std::sort(out.begin(), out.end());
-  out.erase(std::unique(out.begin(), out.end()), out.end());
-}
-
 // Host side of the smoothed-aggregation hierarchy (one-time, mesh-only):
 // aggregates, tentative prolongators from the six rigid-body modes
 // (Solver.jl:117-129), and the patterns of P = (I - w D^-1 A) T, of A P and
-// of the Galerkin operator P^T A P of every level.
+// of the Galerkin operator P^T A P of every level.  Level 0 uses the
+// tangent's block pattern in place (its rowptr/col stay empty).
 void build_amg_structure(pfem_ctx* c) {
   c->hl.clear();
   HostLevel cur;
   cur.nbrow = (int)c->nn;
   cur.bs = 3;
-  cur.rowptr = c->browptr;
-  cur.col = c->bcol;
-  cur.grp = c->browptr;
-  cur.gcl = c->bcol;
   std::vector<double> B;
   double ctr[3] = {0, 0, 0};
   for (long long n = 0; n < c->nn; ++n)
@@ -353,7 +426,11 @@ void build_amg_structure(pfem_ctx* c) {
   for (int lev = 0; lev < 10; ++lev) {
     const int nb = cur.nbrow, bs = cur.bs;
     if ((long long)nb * bs <= 600 && !first) break;
-    cur.nagg = aggregate(nb, cur.grp, cur.gcl, cur.agg);
+    const int* rp = first ? c->browptr.data() : cur.rowptr.data();
+    const int* cl = first ? c->bcol.data() : cur.col.data();
+    const int* grp = first ? rp : cur.grp.data();
+    const int* gcl = first ? cl : cur.gcl.data();
+    cur.nagg = aggregate(nb, grp, gcl, cur.agg);
     if (cur.nagg >= nb || (long long)cur.nagg * 6 >= (long long)nb * bs) break;
     const int na = cur.nagg;
     std::vector<int> aptr(na + 1, 0), amem(nb);
@@ -401,97 +478,60 @@ void build_amg_structure(pfem_ctx* c) {
       for (int i = 0; i < 36; ++i) Bc[(size_t)a * 36 + i] = R[i];
     });
     // P pattern: row n -> aggregates of its matrix neighbours
-    std::vector<std::vector<int>> rows(nb);
+    symbolic_product(nb, rp, cl, nullptr, nullptr, cur.agg.data(), na, cur.p_rp, cur.p_cl);
+    const int nnzP = cur.p_rp[nb];
+    cur.p_row.resize(nnzP);
     par_for(nb, [&](long long n) {
-      auto& v = rows[n];
-      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) v.push_back(cur.agg[cur.col[k]]);
-      sorted_union(v);
+      for (int t = cur.p_rp[n]; t < cur.p_rp[n + 1]; ++t) cur.p_row[t] = (int)n;
     });
-    cur.p_rp.assign(nb + 1, 0);
-    for (int n = 0; n < nb; ++n) cur.p_rp[n + 1] = cur.p_rp[n] + (int)rows[n].size();
-    cur.p_cl.resize(cur.p_rp[nb]);
-    cur.p_row.resize(cur.p_rp[nb]);
-    for (int n = 0; n < nb; ++n)
-      for (size_t t = 0; t < rows[n].size(); ++t) {
-        cur.p_cl[cur.p_rp[n] + t] = rows[n][t];
-        cur.p_row[cur.p_rp[n] + t] = n;
-      }
-    cur.pslot.resize(cur.rowptr[nb]);
+    cur.pslot.resize(rp[nb]);
     par_for(nb, [&](long long n) {
       const int* b0 = cur.p_cl.data() + cur.p_rp[n];
       const int* b1 = cur.p_cl.data() + cur.p_rp[n + 1];
-      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k)
-        cur.pslot[k] = cur.p_rp[n] + (int)(std::lower_bound(b0, b1, cur.agg[cur.col[k]]) - b0);
+      for (int k = rp[n]; k < rp[n + 1]; ++k)
+        cur.pslot[k] = cur.p_rp[n] + (int)(std::lower_bound(b0, b1, cur.agg[cl[k]]) - b0);
     });
     // P^T
     cur.pt_rp.assign(na + 1, 0);
     for (int v : cur.p_cl) cur.pt_rp[v + 1]++;
     for (int a = 0; a < na; ++a) cur.pt_rp[a + 1] += cur.pt_rp[a];
-    cur.pt_blk.resize(cur.p_cl.size());
+    cur.pt_blk.resize(nnzP);
     {
       std::vector<int> f(cur.pt_rp.begin(), cur.pt_rp.end() - 1);
-      for (int p = 0; p < (int)cur.p_cl.size(); ++p) cur.pt_blk[f[cur.p_cl[p]]++] = p;
+      for (int p = 0; p < nnzP; ++p) cur.pt_blk[f[cur.p_cl[p]]++] = p;
     }
     // A P pattern: row n -> union of the P rows of its neighbours
-    par_for(nb, [&](long long n) {
-      std::vector<int> v;
-      for (int k = cur.rowptr[n]; k < cur.rowptr[n + 1]; ++k) {
-        const int m = cur.col[k];
-        v.insert(v.end(), cur.p_cl.begin() + cur.p_rp[m], cur.p_cl.begin() + cur.p_rp[m + 1]);
-      }
-      sorted_union(v);
-      rows[n].swap(v);
-    });
-    cur.ap_rp.assign(nb + 1, 0);
-    for (int n = 0; n < nb; ++n) cur.ap_rp[n + 1] = cur.ap_rp[n] + (int)rows[n].size();
-    cur.ap_cl.resize(cur.ap_rp[nb]);
+    symbolic_product(nb, rp, cl, cur.p_rp.data(), cur.p_cl.data(), nullptr, na, cur.ap_rp, cur.ap_cl);
     cur.ap_row.resize(cur.ap_rp[nb]);
-    for (int n = 0; n < nb; ++n)
-      for (size_t t = 0; t < rows[n].size(); ++t) {
-        cur.ap_cl[cur.ap_rp[n] + t] = rows[n][t];
-        cur.ap_row[cur.ap_rp[n] + t] = n;
-      }
-    rows.clear();
-    // Galerkin pattern of the next level: row I -> union of the AP rows of P^T(I)
-    std::vector<std::vector<int>> crow(na);
-    par_for(na, [&](long long I) {
-      auto& v = crow[I];
-      for (int t = cur.pt_rp[I]; t < cur.pt_rp[I + 1]; ++t) {
-        const int n = cur.p_row[cur.pt_blk[t]];
-        v.insert(v.end(), cur.ap_cl.begin() + cur.ap_rp[n], cur.ap_cl.begin() + cur.ap_rp[n + 1]);
-      }
-      sorted_union(v);
+    par_for(nb, [&](long long n) {
+      for (int t = cur.ap_rp[n]; t < cur.ap_rp[n + 1]; ++t) cur.ap_row[t] = (int)n;
     });
+    // Galerkin pattern of the next level: row I -> union of the AP rows of P^T(I)
     HostLevel nxt;
     nxt.nbrow = na;
     nxt.bs = 6;
-    nxt.rowptr.assign(na + 1, 0);
-    for (int a = 0; a < na; ++a) nxt.rowptr[a + 1] = nxt.rowptr[a] + (int)crow[a].size();
-    nxt.col.resize(nxt.rowptr[na]);
+    {
+      std::vector<int> ptn(nnzP);  // P^T entries as the row of P they come from
+      par_for(nnzP, [&](long long t) { ptn[t] = cur.p_row[cur.pt_blk[t]]; });
+      symbolic_product(na, cur.pt_rp.data(), ptn.data(), cur.ap_rp.data(), cur.ap_cl.data(), nullptr, na,
+                       nxt.rowptr, nxt.col);
+    }
     cur.c_row.resize(nxt.rowptr[na]);
-    for (int a = 0; a < na; ++a)
-      for (size_t t = 0; t < crow[a].size(); ++t) {
-        nxt.col[nxt.rowptr[a] + t] = crow[a][t];
-        cur.c_row[nxt.rowptr[a] + t] = a;
-      }
-    // aggregation graph of the next level: aggregates adjacent in this graph
-    std::vector<std::vector<int>> gadj(na);
     par_for(na, [&](long long a) {
-      auto& v = gadj[a];
-      for (int k = aptr[a]; k < aptr[a + 1]; ++k) {
-        const int n = amem[k];
-        for (int q = cur.grp[n]; q < cur.grp[n + 1]; ++q) v.push_back(cur.agg[cur.gcl[q]]);
-      }
-      sorted_union(v);
+      for (int t = nxt.rowptr[a]; t < nxt.rowptr[a + 1]; ++t) cur.c_row[t] = (int)a;
     });
-    nxt.grp.assign(na + 1, 0);
-    for (int a = 0; a < na; ++a) nxt.grp[a + 1] = nxt.grp[a] + (int)gadj[a].size();
-    nxt.gcl.resize(nxt.grp[na]);
-    for (int a = 0; a < na; ++a) std::copy(gadj[a].begin(), gadj[a].end(), nxt.gcl.begin() + nxt.grp[a]);
+    // aggregation graph of the next level: aggregates adjacent in this graph
+    symbolic_product(na, aptr.data(), amem.data(), grp, gcl, cur.agg.data(), na, nxt.grp, nxt.gcl);
+    cur.grp.clear(); cur.grp.shrink_to_fit();
+    cur.gcl.clear(); cur.gcl.shrink_to_fit();
     c->hl.push_back(std::move(cur));
     cur = std::move(nxt);
     B = std::move(Bc);
     first = false;
+  }
+  if (first) {  // no level was coarsened: the finest level keeps its own pattern copy
+    cur.rowptr = c->browptr;
+    cur.col = c->bcol;
   }
   c->hl.push_back(std::move(cur));  // coarsest: pattern only
   c->amg_struct = true;
@@ -561,7 +601,7 @@ int amg_alloc(pfem_ctx* ctx) {
     AmgLevel<T>& v = A.lv[l];
     v.A.nbrow = h.nbrow;
     v.A.bs = h.bs;
-    v.A.nnzb = h.rowptr[h.nbrow];
+    v.A.nnzb = l == 0 ? ctx->nnzb : h.rowptr[h.nbrow];
     if (l == 0) {
       v.A.rowptr = ctx->dBrowptr;
       v.A.col = ctx->dBcol;
@@ -1321,16 +1361,19 @@ static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t*
   if (what == 0) {
     if (dims) { dims[0] = nr; dims[1] = nr; }
     if (!out) return PFEM_OK;
-    const long long nb = h.rowptr[h.nbrow];
+    // level 0 shares the tangent's block pattern
+    const std::vector<int>& hrp = level == 0 ? ctx->browptr : h.rowptr;
+    const std::vector<int>& hcl = level == 0 ? ctx->bcol : h.col;
+    const long long nb = hrp[h.nbrow];
     std::vector<T> v((size_t)nb * bs * bs);
     const T* src = level < L ? A.lv[level].A.val : A.coarse_val;
     CK(cudaMemcpy(v.data(), src, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
     std::fill(out, out + (size_t)nr * nr, 0.0);
     for (int I = 0; I < h.nbrow; ++I)
-      for (int k = h.rowptr[I]; k < h.rowptr[I + 1]; ++k)
+      for (int k = hrp[I]; k < hrp[I + 1]; ++k)
         for (int r = 0; r < bs; ++r)
           for (int c = 0; c < bs; ++c)
-            out[(size_t)(I * bs + r) * nr + h.col[k] * bs + c] = (double)v[(size_t)k * bs * bs + r * bs + c];
+            out[(size_t)(I * bs + r) * nr + hcl[k] * bs + c] = (double)v[(size_t)k * bs * bs + r * bs + c];
   } else {
     const int nc = h.nagg * 6;
     if (dims) { dims[0] = nr; dims[1] = nc; }
@@ -1371,6 +1414,59 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->max_cuts = 0;
   o->eta_first = 1e-2;
 }
+
+namespace {
+// Block pattern and rank table on the device (topology.cu) for a context with
+// a GPU: fills ctx->browptr / bcol (host copies for the AMG set-up and
+// pfem_pattern) and leaves dElem, dBrowptr, dBcol and dRank on the device.
+// Returns 1, with nothing kept, when a node has more incident elements than
+// the kernel stages; the host path then builds the same pattern.
+int device_pattern(pfem_ctx* ctx, const std::vector<int>& nptr, const std::vector<int>& nel) {
+  const long long nn = ctx->nn, ne = ctx->ne;
+  cudaStream_t st = ctx->st;
+  int *dnptr = nullptr, *dnel = nullptr, *ddeg = nullptr, *derr = nullptr;
+  CK(upload(ctx, &ctx->dElem, ctx->elem));
+  CK(upload(ctx, &dnptr, nptr));
+  CK(upload(ctx, &dnel, nel));
+  CK(dalloc(ctx, &ddeg, (size_t)nn));
+  CK(dalloc(ctx, &derr, 1));
+  CK(cudaMemsetAsync(derr, 0, sizeof(int), st));
+  launch_node_rows((int)nn, dnptr, dnel, ctx->dElem, nullptr, ddeg, nullptr, derr, st);
+  CKL();
+  int herr = 0;
+  std::vector<int> deg(nn);
+  CK(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(deg.data(), ddeg, nn * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  auto release = [&]() {
+    dfree(ctx, dnptr); dfree(ctx, dnel); dfree(ctx, ddeg); dfree(ctx, derr);
+  };
+  if (herr) {
+    release();
+    dfree(ctx, ctx->dElem);
+    return 1;
+  }
+  ctx->browptr.assign(nn + 1, 0);
+  long long acc = 0;
+  for (long long n = 0; n < nn; ++n) {
+    acc += deg[n];
+    if (acc * 9 >= (1ll << 31)) return fail(ctx, PFEM_ERR_BAD_ARG, "pattern too large for 32-bit indices");
+    ctx->browptr[n + 1] = (int)acc;
+  }
+  CK(upload(ctx, &ctx->dBrowptr, ctx->browptr));
+  CK(dalloc(ctx, &ctx->dBcol, (size_t)acc));
+  launch_node_rows((int)nn, dnptr, dnel, ctx->dElem, ctx->dBrowptr, nullptr, ctx->dBcol, derr, st);
+  CKL();
+  CK(dalloc(ctx, &ctx->dRank, (size_t)ne * 64));
+  launch_rank_table(ne, ctx->dElem, ctx->dBrowptr, ctx->dBcol, ctx->dRank, st);
+  CKL();
+  ctx->bcol.resize(acc);
+  CK(cudaMemcpyAsync(ctx->bcol.data(), ctx->dBcol, acc * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  release();
+  return PFEM_OK;
+}
+}  // namespace
 
 const char* pfem_last_error(const pfem_ctx* ctx) {
   if (!ctx) return g_cuda_err.c_str();
@@ -1454,34 +1550,67 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     for (int64_t e = 0; e < ne; ++e)
       for (int a = 0; a < 8; ++a) nel[f[ctx->elem[e * 8 + a]]++] = (int)e;
   }
-  std::vector<int> deg(nn);
-  std::vector<std::vector<int>> adj(nn);
-  par_for(nn, [&](long long n) {
-    std::vector<int>& v = adj[n];
-    v.reserve(64);
-    for (int k = nptr[n]; k < nptr[n + 1]; ++k)
-      for (int b = 0; b < 8; ++b) v.push_back(ctx->elem[(long long)nel[k] * 8 + b]);
-    std::sort(v.begin(), v.end());
-    v.erase(std::unique(v.begin(), v.end()), v.end());
-    deg[n] = (int)v.size();
-  });
-  ctx->browptr.assign(nn + 1, 0);
-  for (int64_t n = 0; n < nn; ++n) ctx->browptr[n + 1] = ctx->browptr[n] + deg[n];
-  ctx->nnzb = ctx->browptr[nn];
-  if (ctx->nnzb * 9 >= (1ll << 31)) return bail(fail(ctx, PFEM_ERR_BAD_ARG, "pattern too large for 32-bit indices"));
-  ctx->bcol.resize(ctx->nnzb);
-  par_for(nn, [&](long long n) { std::copy(adj[n].begin(), adj[n].end(), ctx->bcol.begin() + ctx->browptr[n]); });
-  std::vector<uint8_t> rank((size_t)ne * 64);
-  par_for(ne, [&](long long e) {
-    for (int a = 0; a < 8; ++a) {
-      const auto& v = adj[ctx->elem[e * 8 + a]];
-      for (int b = 0; b < 8; ++b)
-        rank[(size_t)e * 64 + a * 8 + b] =
-            (uint8_t)(std::lower_bound(v.begin(), v.end(), ctx->elem[e * 8 + b]) - v.begin());
+  // block pattern: row n = sorted, distinct nodes of the elements incident to
+  // n (Assembly.jl:62-82, :99-111).  With a GPU it is built on the device
+  // (topology.cu); topology-only contexts, and meshes with a node in more than
+  // 64 elements, build it here: two passes (count, fill) over rows of a few
+  // dozen entries with one reused buffer per thread.
+  bool dev_pattern = false;
+  if (device >= 0) {
+    const int rc = device_pattern(ctx, nptr, nel);
+    if (rc < 0) return bail(rc);
+    dev_pattern = rc == PFEM_OK;
+  }
+  if (!dev_pattern) {
+    ctx->browptr.assign(nn + 1, 0);
+    auto node_row = [&](long long n, std::vector<int>& buf) {
+      buf.clear();
+      for (int k = nptr[n]; k < nptr[n + 1]; ++k)
+        for (int b = 0; b < 8; ++b) buf.push_back(ctx->elem[(long long)nel[k] * 8 + b]);
+      std::sort(buf.begin(), buf.end());
+      buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+    };
+    par_chunks(nn, [&](long long b, long long e) {
+      std::vector<int> buf;
+      for (long long n = b; n < e; ++n) {
+        node_row(n, buf);
+        ctx->browptr[n + 1] = (int)buf.size();
+      }
+    });
+    long long acc = 0;
+    for (int64_t n = 0; n < nn; ++n) {
+      acc += ctx->browptr[n + 1];
+      if (acc * 9 >= (1ll << 31)) return bail(fail(ctx, PFEM_ERR_BAD_ARG, "pattern too large for 32-bit indices"));
+      ctx->browptr[n + 1] = (int)acc;
     }
-  });
-  adj.clear();
-  adj.shrink_to_fit();
+    ctx->bcol.resize(ctx->browptr[nn]);
+    par_chunks(nn, [&](long long b, long long e) {
+      std::vector<int> buf;
+      for (long long n = b; n < e; ++n) {
+        node_row(n, buf);
+        std::copy(buf.begin(), buf.end(), ctx->bcol.begin() + ctx->browptr[n]);
+      }
+    });
+  }
+  ctx->nnzb = ctx->browptr[nn];
+  for (int64_t n = 0; n < nn; ++n)
+    if (ctx->browptr[n + 1] - ctx->browptr[n] > 256)
+      return bail(fail(ctx, PFEM_ERR_BAD_ARG, "a node has more than 256 neighbours (8-bit rank table)"));
+  // rank[e][a][b] = position of node b in node a's block row (host path only;
+  // the device path built it in place)
+  std::vector<uint8_t> rank;
+  if (!dev_pattern && device >= 0) {
+    rank.resize((size_t)ne * 64);
+    par_for(ne, [&](long long e) {
+      for (int a = 0; a < 8; ++a) {
+        const int na_ = ctx->elem[e * 8 + a];
+        const int* b0 = ctx->bcol.data() + ctx->browptr[na_];
+        const int* b1 = ctx->bcol.data() + ctx->browptr[na_ + 1];
+        for (int b = 0; b < 8; ++b)
+          rank[(size_t)e * 64 + a * 8 + b] = (uint8_t)(std::lower_bound(b0, b1, ctx->elem[e * 8 + b]) - b0);
+      }
+    });
+  }
   // colors: the reference's rule is reported; the device uses it when it
   // yields independent sets (> 1 color), else a greedy coloring.
   ctx->ncolors_ref = reference_colors(ctx->X, nn, ne, ctx->color_ref);
@@ -1517,10 +1646,12 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
 #define UP(ptr, vec) if ((ce = upload(ctx, &ptr, vec)) != cudaSuccess) { pfem_set_cuda_error(ce, #ptr, __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
 #define AL(ptr, n) if ((ce = dalloc(ctx, &ptr, n)) != cudaSuccess) { pfem_set_cuda_error(ce, #ptr, __FILE__, __LINE__); return bail(PFEM_ERR_CUDA); }
   UP(ctx->dX, ctx->X);
-  UP(ctx->dElem, ctx->elem);
-  UP(ctx->dRank, rank);
-  UP(ctx->dBrowptr, ctx->browptr);
-  UP(ctx->dBcol, ctx->bcol);
+  if (!dev_pattern) {
+    UP(ctx->dElem, ctx->elem);
+    UP(ctx->dRank, rank);
+    UP(ctx->dBrowptr, ctx->browptr);
+    UP(ctx->dBcol, ctx->bcol);
+  }
   UP(ctx->dColorList, clist);
   UP(ctx->dAllElems, all);
   if (sigy0_e) {

@@ -40,6 +40,13 @@ template <typename KT>
 void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, int hard,
                           cudaStream_t st);
 
+// One-time topology on the device (topology.cu): per-node block rows
+// (count pass with col = null, fill pass with rowptr) and the rank table.
+void launch_node_rows(int nn, const int* nptr, const int* nel, const int* elem, const int* rowptr, int* deg,
+                      int* col, int* err, cudaStream_t st);
+void launch_rank_table(long long ne, const int* elem, const int* rowptr, const int* col, uint8_t* rank,
+                       cudaStream_t st);
+
 // ---------------- block-CSR matrices ----------------
 template <typename VT>
 struct BsrMat {
