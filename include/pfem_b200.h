@@ -80,7 +80,11 @@ typedef struct pfem_solve_opts {
   double eta_min, eta_max, ew_gamma, ew_alpha;
   int32_t krylov_itmax;  /* cg_itmax */
   int32_t predictor;     /* pfem_predictor */
-  int32_t amg_rebuild;   /* 0: once per load step (reference policy); 1: every Newton iteration */
+  int32_t amg_rebuild;   /* 0: once per load step (reference policy); 1: every Newton iteration;
+                            2 (default): adaptive -- keep the numeric hierarchy across load
+                            steps and rebuild when a Krylov solve needs more than
+                            amg_stale_ratio times the iterations per decade of the first solve
+                            after the last rebuild (or after reset / a new constrained set) */
   int32_t cheb_degree;   /* Chebyshev smoother degree */
   int32_t verbose;
   int32_t line_search;   /* 0: full Newton steps (the reference); 1: backtrack (halving, at
@@ -98,6 +102,7 @@ typedef struct pfem_solve_opts {
                             converged yet (the first increment, from U = 0 and the full
                             boundary-value jump), the inner tolerance is capped at eta_first;
                             <= 0 = the reference's forcing term throughout */
+  double amg_stale_ratio; /* amg_rebuild = 2 only (default 1.5) */
 } pfem_solve_opts;
 
 typedef struct pfem_solve_result {

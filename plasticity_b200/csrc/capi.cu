@@ -127,6 +127,10 @@ struct pfem_ctx {
   // learned predictor
   pfem::MlpState mlp;
   int steps_taken = 0;
+  // adaptive AMG reuse (amg_rebuild = 2): Krylov iterations per decade of the
+  // first solve after the last rebuild, and whether a later solve exceeded it
+  double amg_ipd_base = -1.0;
+  bool amg_stale = true;
   double lam_prev = 0.0, lam_prev2 = 0.0, lam_prev3 = 0.0;
 };
 
@@ -1161,7 +1165,7 @@ int residual_system(pfem_ctx* ctx, int prec, double lam, double* rnorm, double* 
 // Solve K dU = -R (device R) with precision prec; the correction stays in
 // the precision-T Krylov vector kw.x.
 int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool rebuild, int* kits,
-                      double* t_amg, double* t_kry) {
+                      double* t_amg, double* t_kry, bool* converged = nullptr) {
   const int prec = o->precision;
   int rc;
   auto t0 = std::chrono::steady_clock::now();
@@ -1196,7 +1200,8 @@ int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool
   CK(cudaStreamSynchronize(ctx->st));
   auto t2 = std::chrono::steady_clock::now();
   *t_kry += std::chrono::duration<double, std::milli>(t2 - t1).count();
-  (void)conv;  // an inexact inner solve is still a descent step; Newton judges it
+  // an inexact inner solve is still a descent step; Newton judges it
+  if (converged) *converged = conv;
   return PFEM_OK;
 }
 
@@ -1254,11 +1259,30 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     // first direction there sends the line search into a long damped sequence
     // (measured at 64^3-100^3: 33-50 Newton iterations at eta_max = 0.1, 5-18 at 1e-2).
     if (o->lin_rtol <= 0 && o->eta_first > 0 && ctx->steps_taken == 0) eta = std::min(eta, o->eta_first);
-    const bool rebuild = first || o->amg_rebuild;
+    bool rebuild = o->amg_rebuild == 2 ? ctx->amg_stale : (first || o->amg_rebuild);
     first = false;
     int kits = 0;
-    rc = newton_correction(ctx, o, eta, rebuild, &kits, &tm->amg_ms, &tm->kry_ms);
+    bool kconv = true;
+    rc = newton_correction(ctx, o, eta, rebuild, &kits, &tm->amg_ms, &tm->kry_ms, &kconv);
     if (rc) return rc;
+    if (o->amg_rebuild == 2 && !rebuild && !kconv) {
+      // a reused hierarchy that no longer reaches the tolerance: rebuild and solve again,
+      // so the adaptive policy never takes a worse direction than the per-step rebuild
+      tm->kits += kits;
+      rebuild = true;
+      rc = newton_correction(ctx, o, eta, true, &kits, &tm->amg_ms, &tm->kry_ms, &kconv);
+      if (rc) return rc;
+    }
+    if (o->amg_rebuild == 2) {
+      // iterations per decade of residual reduction asked of this solve
+      const double ipd = kits / std::max(std::log10(1.0 / eta), 0.5);
+      if (rebuild) {
+        ctx->amg_ipd_base = ipd;
+        ctx->amg_stale = false;
+      } else if (kits > o->amg_stale_ratio * ctx->amg_ipd_base * std::max(std::log10(1.0 / eta), 0.5) + 2) {
+        ctx->amg_stale = true;
+      }
+    }
     if (khist) khist[it - 1] = kits;
     tm->kits += kits;
     rkm1 = rn;
@@ -1406,13 +1430,14 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->ew_alpha = 1.5;
   o->krylov_itmax = 200;
   o->predictor = PFEM_PRED_PREVIOUS;
-  o->amg_rebuild = 0;
+  o->amg_rebuild = 2;
   o->cheb_degree = 2;
   o->verbose = 0;
   o->line_search = 0;
   o->predictor_smooth = 16;
   o->max_cuts = 0;
   o->eta_first = 1e-2;
+  o->amg_stale_ratio = 1.5;
 }
 
 namespace {
@@ -1850,6 +1875,7 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   CK(upload(ctx, &b.zone, zone));
   ctx->bc_dofs = dofs;
   ctx->bcs_set = true;
+  ctx->amg_stale = true;  // a new constrained set changes the imposed tangent's structure
   return PFEM_OK;
 }
 
@@ -1867,6 +1893,7 @@ int pfem_reset(pfem_ctx* ctx) {
   CK(cudaMemsetAsync(ctx->dUprev3, 0, ctx->ndof * sizeof(double), ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   ctx->steps_taken = 0;
+  ctx->amg_stale = true;
   ctx->mlp.used_count = 0;
   ctx->mlp.have_feat = false;
   ctx->lam_prev = ctx->lam_prev2 = ctx->lam_prev3 = 0.0;
