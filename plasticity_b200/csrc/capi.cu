@@ -101,6 +101,7 @@ struct pfem_ctx {
   int* dAllElems = nullptr;
   double *dCpi = nullptr, *dAlpha = nullptr, *dEpsp = nullptr, *dTau = nullptr;
   double* dBeta = nullptr;  // 6 x ngp committed back stress, kinematic hardening only
+  double* dOut = nullptr;   // 6 x ngp scratch for per-GP results in the caller's layout (lazy)
   int hard = HARD_LINEAR;   // hardening law of the element kernels
   uint8_t* dFlags = nullptr;
   double *dU = nullptr, *dR = nullptr, *dDg = nullptr, *dUprev = nullptr, *dUprev2 = nullptr;
@@ -2314,6 +2315,73 @@ int pfem_amg_dense(pfem_ctx* ctx, int32_t level, int32_t what, double* out, int6
   return amg_dense_t<double>(ctx, level, what, out, dims);
 }
 
+namespace {
+// Component-major device state (c * ngp + gp) to the caller's per-GP layout
+// (gp * 6 + c), optionally divided by a per-GP factor.
+__global__ void soa_to_aos_kernel(long long ngp, const double* __restrict__ src, double* __restrict__ dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ngp * 6; i += (long long)gridDim.x * blockDim.x) {
+    const long long g = i / 6;
+    const int c = (int)(i - g * 6);
+    dst[i] = src[(long long)c * ngp + g];
+  }
+}
+
+// Cauchy stress tau / det F with the standard F at every Gauss point
+// (gauss_stress, Model.jl:188-208), one thread per Gauss point, written in the
+// caller's per-GP layout.  det F <= 0 leaves tau unscaled, as the host rule did.
+__global__ void cauchy_kernel(long long ne, const double* __restrict__ X, const int* __restrict__ elem,
+                              const double* __restrict__ U, const double* __restrict__ tau,
+                              double* __restrict__ out) {
+  const long long ngp = ne * 8;
+  const double gc = 0.57735026918962576451;
+  for (long long gp = blockIdx.x * (long long)blockDim.x + threadIdx.x; gp < ngp; gp += (long long)gridDim.x * blockDim.x) {
+    const long long e = gp >> 3;
+    const int g = (int)(gp & 7);
+    const double sgx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sgy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
+                 sgz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+    const double xi = sgx[g] * gc, et = sgy[g] * gc, ze = sgz[g] * gc;
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const double d0 = 0.125 * sgx[a] * (1 + sgy[a] * et) * (1 + sgz[a] * ze);
+      const double d1 = 0.125 * sgy[a] * (1 + sgx[a] * xi) * (1 + sgz[a] * ze);
+      const double d2 = 0.125 * sgz[a] * (1 + sgx[a] * xi) * (1 + sgy[a] * et);
+      const long long n = elem[e * 8 + a];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double x = X[n * 3 + i], u = U[n * 3 + i];
+        J[3 * i] += x * d0; J[3 * i + 1] += x * d1; J[3 * i + 2] += x * d2;
+        H[3 * i] += u * d0; H[3 * i + 1] += u * d1; H[3 * i + 2] += u * d2;
+      }
+    }
+    double Ji[9], F[9];
+    pfem::inv3(J, Ji);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        F[3 * i + j] = (i == j ? 1.0 : 0.0) + H[3 * i] * Ji[j] + H[3 * i + 1] * Ji[3 + j] + H[3 * i + 2] * Ji[6 + j];
+    const double dF = pfem::det3(F);
+    const double inv = dF > 0 ? 1.0 / dF : 1.0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) out[gp * 6 + c] = tau[(long long)c * ngp + gp] * inv;
+  }
+}
+
+// Copy a component-major 6 x ngp device array to a host buffer in per-GP
+// layout through the device scratch (one transpose on the device, one copy).
+int download_aos(pfem_ctx* ctx, const double* d, double* h) {
+  const long long ngp = ctx->ngp;
+  if (!ctx->dOut) CK(dalloc(ctx, &ctx->dOut, (size_t)6 * ngp));
+  pfem::count_launch();
+  soa_to_aos_kernel<<<1024, 256, 0, ctx->st>>>(ngp, d, ctx->dOut);
+  CKL();
+  CK(cudaMemcpyAsync(h, ctx->dOut, (size_t)6 * ngp * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return PFEM_OK;
+}
+}  // namespace
+
 int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, double* cpi, double* epsp,
                    uint8_t* flags) {
   if (!ctx) return PFEM_ERR_BAD_ARG;
@@ -2322,20 +2390,12 @@ int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, d
   cudaSetDevice(ctx->device);
   if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return PFEM_ERR_CUDA;
   const long long ngp = ctx->ngp;
-  auto soa = [&](const double* d, double* h) -> int {
-    std::vector<double> t(6 * ngp);
-    if (cudaMemcpy(t.data(), d, 6 * ngp * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
-    for (long long g = 0; g < ngp; ++g)
-      for (int k = 0; k < 6; ++k) h[g * 6 + k] = t[k * ngp + g];
-    return PFEM_OK;
-  };
   if (U && cudaMemcpy(U, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
   if (alpha && cudaMemcpy(alpha, ctx->dAlpha, ngp * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
   if (flags && cudaMemcpy(flags, ctx->dFlags, ngp, cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
-  if (tau && soa(ctx->dTau, tau)) return PFEM_ERR_CUDA;
-  if (cpi && soa(ctx->dCpi, cpi)) return PFEM_ERR_CUDA;
-  if (epsp && soa(ctx->dEpsp, epsp)) return PFEM_ERR_CUDA;
-  (void)c;
+  if (tau && download_aos(c, ctx->dTau, tau)) return PFEM_ERR_CUDA;
+  if (cpi && download_aos(c, ctx->dCpi, cpi)) return PFEM_ERR_CUDA;
+  if (epsp && download_aos(c, ctx->dEpsp, epsp)) return PFEM_ERR_CUDA;
   return PFEM_OK;
 }
 
@@ -2343,41 +2403,24 @@ int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma) {
   if (!ctx || !sigma) return PFEM_ERR_BAD_ARG;
   // the small-strain kind stores sigma itself (Model.jl:188-208, small branch)
   if (ctx->kind == PFEM_HEX8_SMALL) return pfem_get_state(ctx, nullptr, sigma, nullptr, nullptr, nullptr, nullptr);
-  // tau / det F at each Gauss point with the standard F (Model.jl:188-208)
-  std::vector<double> U(ctx->ndof);
-  int rc = pfem_get_state(ctx, U.data(), sigma, nullptr, nullptr, nullptr, nullptr);
-  if (rc) return rc;
-  const double gc = 1.0 / std::sqrt(3.0);
-  static const int sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
-                   sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
-  par_for(ctx->ne, [&](long long e) {
-    for (int g = 0; g < 8; ++g) {
-      const double xi = sx[g] * gc, et = sy[g] * gc, ze = sz[g] * gc;
-      double J[9] = {0}, H[9] = {0};
-      for (int a = 0; a < 8; ++a) {
-        const double d0 = 0.125 * sx[a] * (1 + sy[a] * et) * (1 + sz[a] * ze);
-        const double d1 = 0.125 * sy[a] * (1 + sx[a] * xi) * (1 + sz[a] * ze);
-        const double d2 = 0.125 * sz[a] * (1 + sx[a] * xi) * (1 + sy[a] * et);
-        const int n = ctx->elem[e * 8 + a];
-        for (int i = 0; i < 3; ++i) {
-          J[3 * i] += ctx->X[n * 3 + i] * d0; J[3 * i + 1] += ctx->X[n * 3 + i] * d1; J[3 * i + 2] += ctx->X[n * 3 + i] * d2;
-          H[3 * i] += U[n * 3 + i] * d0; H[3 * i + 1] += U[n * 3 + i] * d1; H[3 * i + 2] += U[n * 3 + i] * d2;
-        }
-      }
-      const double dJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
-      double Ji[9];
-      Ji[0] = (J[4] * J[8] - J[5] * J[7]) / dJ; Ji[1] = (J[2] * J[7] - J[1] * J[8]) / dJ; Ji[2] = (J[1] * J[5] - J[2] * J[4]) / dJ;
-      Ji[3] = (J[5] * J[6] - J[3] * J[8]) / dJ; Ji[4] = (J[0] * J[8] - J[2] * J[6]) / dJ; Ji[5] = (J[2] * J[3] - J[0] * J[5]) / dJ;
-      Ji[6] = (J[3] * J[7] - J[4] * J[6]) / dJ; Ji[7] = (J[1] * J[6] - J[0] * J[7]) / dJ; Ji[8] = (J[0] * J[4] - J[1] * J[3]) / dJ;
-      double F[9];
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-          F[3 * i + j] = (i == j ? 1.0 : 0.0) + H[3 * i] * Ji[j] + H[3 * i + 1] * Ji[3 + j] + H[3 * i + 2] * Ji[6 + j];
-      const double dF = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) + F[2] * (F[3] * F[7] - F[4] * F[6]);
-      const double inv = dF > 0 ? 1.0 / dF : 1.0;
-      for (int k = 0; k < 6; ++k) sigma[(e * 8 + g) * 6 + k] *= inv;
-    }
-  });
+  if (ctx->device < 0) return PFEM_ERR_STATE;
+  pfem_ctx* c = const_cast<pfem_ctx*>(ctx);
+  cudaSetDevice(ctx->device);
+  // tau / det F at each Gauss point with the standard F (Model.jl:188-208), on the device
+  if (!c->dOut) {
+    const cudaError_t e__ = dalloc(c, &c->dOut, (size_t)6 * ctx->ngp);
+    if (e__ != cudaSuccess) { pfem_set_cuda_error(e__, "dOut", __FILE__, __LINE__); return cuda_fail(c); }
+  }
+  pfem::count_launch();
+  cauchy_kernel<<<1024, 256, 0, ctx->st>>>(ctx->ne, ctx->dX, ctx->dElem, ctx->dU, ctx->dTau, c->dOut);
+  {
+    cudaError_t e__ = cudaGetLastError();
+    if (e__ != cudaSuccess) { pfem_set_cuda_error(e__, "kernel launch", __FILE__, __LINE__); return cuda_fail(c); }
+  }
+  if (cudaMemcpyAsync(sigma, c->dOut, (size_t)6 * ctx->ngp * sizeof(double), cudaMemcpyDeviceToHost, ctx->st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(ctx->st) != cudaSuccess)
+    return PFEM_ERR_CUDA;
   return PFEM_OK;
 }
 

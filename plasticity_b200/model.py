@@ -507,17 +507,22 @@ def nodal_displacements(model) -> np.ndarray:
 
 
 def gauss_kirchhoff(model) -> np.ndarray:
-    """Committed Kirchhoff stress, 6 x ngp (Model.jl:227)."""
-    return model.state()["tau"].T.copy()
+    """Committed Kirchhoff stress, 6 x ngp (Model.jl:227); a view of the per-GP
+    (ngp, 6) array the library fills."""
+    t = np.zeros((model.ngp, 6))
+    check(L.lib().pfem_get_state(model._ctx, None, ptr(t), None, None, None, None), model._ctx)
+    return t.T
 
 
 def gauss_stress(model) -> np.ndarray:
     """Cauchy stress tau / det F (standard F), 6 x ngp (Model.jl:188-208)."""
     s = np.zeros((model.ngp, 6))
     check(L.lib().pfem_gauss_stress(model._ctx, ptr(s)), model._ctx)
-    return s.T.copy()
+    return s.T
 
 
 def equivalent_plastic_strain(model) -> np.ndarray:
     """Committed equivalent plastic strain alpha per GP (Model.jl:232)."""
-    return model.state()["alpha"]
+    a = np.zeros(model.ngp)
+    check(L.lib().pfem_get_state(model._ctx, None, None, ptr(a), None, None, None), model._ctx)
+    return a
