@@ -707,14 +707,26 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
         for (int i = 0; i < 3; ++i) acc[a * 3 + i] += x0 * T[i] + x1 * T[3 + i] + x2 * T[6 + i];
       }
     }
+    // The eight target blocks lie in eight different block rows, so nothing
+    // aliases: all 24 loads are issued before any store (one memory latency
+    // per column instead of a chain of eight).
     const int* nds = nodes_s[warp][s];
+    KT* vp[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      vp[a] = p.Kval + ((long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b]) * 9 + k;
+    KT old[24];
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
-      const long long blk = (long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b];
-      KT* v = p.Kval + blk * 9 + k;
-      v[0] += (KT)acc[a * 3 + 0];
-      v[3] += (KT)acc[a * 3 + 1];
-      v[6] += (KT)acc[a * 3 + 2];
+      old[a * 3 + 0] = vp[a][0];
+      old[a * 3 + 1] = vp[a][3];
+      old[a * 3 + 2] = vp[a][6];
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      vp[a][0] = old[a * 3 + 0] + (KT)acc[a * 3 + 0];
+      vp[a][3] = old[a * 3 + 1] + (KT)acc[a * 3 + 1];
+      vp[a][6] = old[a * 3 + 2] + (KT)acc[a * 3 + 2];
     }
   }
   }  // !COMMIT
@@ -961,13 +973,22 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
         }
       }
       const int* nds = nodes_s[warp][s2];
+      KT* vp[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+        vp[a] = p.Kval + ((long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b]) * 9 + k;
+      KT old[24];
 #pragma unroll
       for (int a = 0; a < 8; ++a) {
-        const long long blk = (long long)p.browptr[nds[a]] + p.rank[(long long)es * 64 + a * 8 + b];
-        KT* v = p.Kval + blk * 9 + k;
-        v[0] += (KT)acc[a * 3 + 0];
-        v[3] += (KT)acc[a * 3 + 1];
-        v[6] += (KT)acc[a * 3 + 2];
+        old[a * 3 + 0] = vp[a][0];
+        old[a * 3 + 1] = vp[a][3];
+        old[a * 3 + 2] = vp[a][6];
+      }
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        vp[a][0] = old[a * 3 + 0] + (KT)acc[a * 3 + 0];
+        vp[a][3] = old[a * 3 + 1] + (KT)acc[a * 3 + 1];
+        vp[a][6] = old[a * 3 + 2] + (KT)acc[a * 3 + 2];
       }
     }
   }
