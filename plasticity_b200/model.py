@@ -201,28 +201,35 @@ class Model:
         comp = comp.lstrip(":")
         return {"x": (1,), "y": (2,), "z": (3,), "all": (1, 2, 3)}[comp]
 
+    def _dofs(self, nodes, comp):
+        """1-based dofs of `nodes` x `comp`, node-major (the order of the
+        reference builders' nested loops)."""
+        nodes = np.atleast_1d(np.asarray(nodes, np.int64))
+        comps = np.asarray(self._comps(comp), np.int64)
+        return (3 * (nodes[:, None] - 1) + comps[None, :]).reshape(-1)
+
+    def _extend(self, **arrays):
+        # the lists may be numpy arrays (Workload.apply assigns arrays)
+        for name, add in arrays.items():
+            cur = getattr(self, name)
+            setattr(self, name, np.concatenate([np.asarray(cur, add.dtype), add]))
+
     def fix(self, nodes, comp="all"):
-        for n in np.atleast_1d(nodes):
-            for c in self._comps(comp):
-                self.dir_dofs.append(3 * (int(n) - 1) + c); self.dir_vals.append(0.0); self.dir_ramp.append(0)
-        self._bcs_dirty = True
+        d = self._dofs(nodes, comp)
+        self._extend(dir_dofs=d, dir_vals=np.zeros(len(d)), dir_ramp=np.zeros(len(d), np.uint8))
         return self
 
     def prescribe(self, nodes, comp, value, ramp=True):
-        for n in np.atleast_1d(nodes):
-            for c in self._comps(comp):
-                self.dir_dofs.append(3 * (int(n) - 1) + c); self.dir_vals.append(float(value))
-                self.dir_ramp.append(1 if ramp else 0)
-        self._bcs_dirty = True
+        d = self._dofs(nodes, comp)
+        self._extend(dir_dofs=d, dir_vals=np.full(len(d), float(value)),
+                     dir_ramp=np.full(len(d), 1 if ramp else 0, np.uint8))
         return self
 
     def load(self, nodes, comp, value, distribute=False):
         nodes = np.atleast_1d(nodes)
         per = float(value) / len(nodes) if distribute else float(value)
-        for n in nodes:
-            for c in self._comps(comp):
-                self.neu_dofs.append(3 * (int(n) - 1) + c); self.neu_vals.append(per)
-        self._bcs_dirty = True
+        d = self._dofs(nodes, comp)
+        self._extend(neu_dofs=d, neu_vals=np.full(len(d), per))
         return self
 
     def _push_bcs(self):
@@ -502,8 +509,9 @@ def reset(model):
 
 
 def nodal_displacements(model) -> np.ndarray:
-    """nodal_displacements (Model.jl:169-178): 3 x nn."""
-    return model.U.reshape(-1, 3).T.copy()
+    """nodal_displacements (Model.jl:169-178): 3 x nn, a view of the node-major
+    displacement vector (the reference's column-major 3 x nn layout)."""
+    return model.U.reshape(-1, 3).T
 
 
 def gauss_kirchhoff(model) -> np.ndarray:

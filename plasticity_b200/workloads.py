@@ -39,12 +39,14 @@ class Workload:
     meta: dict = field(default_factory=dict)
 
     def apply(self, model):
-        """Push the BCs into a Model (product or oracle: both expose fix/prescribe lists)."""
-        model.dir_dofs = list(map(int, self.dir_dofs))
-        model.dir_vals = list(map(float, self.dir_vals))
-        model.dir_ramp = list(map(int, self.dir_ramp))
-        model.neu_dofs = list(map(int, self.neu_dofs))
-        model.neu_vals = list(map(float, self.neu_vals))
+        """Push the BCs into a Model: arrays for the product model, lists for the
+        oracle's (whose builders append)."""
+        conv = (lambda a, t: np.array(a, t)) if hasattr(model, "_bcs_dirty") else (lambda a, t: np.array(a, t).tolist())
+        model.dir_dofs = conv(self.dir_dofs, np.int64)
+        model.dir_vals = conv(self.dir_vals, np.float64)
+        model.dir_ramp = conv(self.dir_ramp, np.uint8)
+        model.neu_dofs = conv(self.neu_dofs, np.int64)
+        model.neu_vals = conv(self.neu_vals, np.float64)
         if hasattr(model, "_bcs_dirty"):
             model._bcs_dirty = True
         return model
