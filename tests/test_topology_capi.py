@@ -143,3 +143,28 @@ def test_boundary_condition_changes_mark_model_dirty():
     M._bcs_dirty = False
     M.prescribe([1], "x", 0.1)
     assert M._bcs_dirty
+
+
+def test_bc_builders_match_oracle_loops(oracle):
+    """fix!/prescribe!/load! (Model.jl:102-145): the vectorised builders give the
+    oracle's node-major dof order, values and ramp flags; after Workload.apply
+    (arrays) further builder calls extend the arrays."""
+    mesh = P.box_mesh(1.0, 2.0, 1.0, 3, 2, 2)
+    M = P.Model(mesh, MAT, device=-1)
+    om = oracle.OracleModel(mesh.nodes, mesh.elements, oracle.J2Material(210e3, 0.3, 250.0, 1000.0))
+    for m in (M, om):
+        m.fix(P.on_face(mesh, "zmin"), "all")
+        m.fix(P.on_face(mesh, "xmin"), "x")
+        m.prescribe(P.on_face(mesh, "xmax"), "y", -0.02)
+        m.prescribe(P.on_face(mesh, "zmax"), "z", 0.01, ramp=False)
+        m.load(P.on_face(mesh, "ymax"), "x", 6.0, distribute=True)
+    assert np.array_equal(np.asarray(M.dir_dofs), np.asarray(om.dir_dofs))
+    assert np.array_equal(np.asarray(M.dir_vals), np.asarray(om.dir_vals))
+    assert np.array_equal(np.asarray(M.dir_ramp, bool), np.asarray(om.dir_ramp, bool))
+    assert np.array_equal(np.asarray(M.neu_dofs), np.asarray(om.neu_dofs))
+    assert np.allclose(np.asarray(M.neu_vals), np.asarray(om.neu_vals), rtol=0, atol=0)
+    w = W.config2(n=3)
+    w.apply(M)
+    n0 = len(M.dir_dofs)
+    M.fix([1], "z")
+    assert len(M.dir_dofs) == n0 + 1 and M.dir_dofs[-1] == 3 and M._bcs_dirty
