@@ -217,7 +217,7 @@ int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, d
 int pfem_set_state(pfem_ctx* ctx, const double* cpi, const double* alpha, const double* epsp);
 /* Overwrite U (host ndof) -- e.g. to evaluate a predictor guess. */
 int pfem_set_displacement(pfem_ctx* ctx, const double* U);
-/* Committed back stress beta (state_committed.beta, Model.jl:53-60), 6 x ngp
+/* Committed back stress beta (state_committed.beta: Model.jl:38, GaussState Mesh.jl:124-130), 6 x ngp
  * column-major (physical-shear Voigt).  For the finite kinds it is the
  * rotation-neutralised back stress of the reference configuration
  * (FiniteStrain.jl:292-346).  get writes zeros when Hkin = 0; set needs
