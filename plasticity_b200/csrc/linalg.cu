@@ -435,8 +435,10 @@ void impose_dirichlet(const BcDev& bc, long long ndof, double lam, const double*
   pfem::count_launch(); residual_fext_kernel<<<b1, 256, 0, st>>>(ndof, lam, bc.fn, R);
   if (bc.nbc == 0) return;
   pfem::count_launch(); bc_dg_kernel<<<(bc.nbc + 255) / 256, 256, 0, st>>>(bc.nbc, bc.dofs, bc.vals, bc.ramp, lam, U, dg);
-  if (bc.nrows > 0)
-    pfem::count_launch(); bc_rhs_kernel<KT><<<(bc.nrows + 127) / 128, 128, 0, st>>>(bc.nrows, bc.rows, bc.rptr, bc.rpos, bc.rcol, K, dg, R);
+  if (bc.nrows > 0) {  // none when every dof is constrained
+    pfem::count_launch();
+    bc_rhs_kernel<KT><<<(bc.nrows + 127) / 128, 128, 0, st>>>(bc.nrows, bc.rows, bc.rptr, bc.rpos, bc.rcol, K, dg, R);
+  }
   if (bc.nzero > 0) {
     const int b2 = (int)std::min<long long>((bc.nzero + 255) / 256, 4096);
     pfem::count_launch(); bc_zero_kernel<KT><<<b2, 256, 0, st>>>(bc.nzero, bc.zpos, bc.zone, K);

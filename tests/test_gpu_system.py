@@ -60,9 +60,10 @@ def test_T14_cantilever_vs_beam_theory_and_oracle(oracle):
         M = P.Model(mesh, P.J2Material(E, NU, 1e9), element="small")
         M.fix(P.on_face(mesh, "xmin"), "all")
         M.load(P.on_face(mesh, "xmax"), "z", -Pz, distribute=True)
-        # near-exact inner solves and a tight Newton tolerance, so the displacement
-        # itself (not only the residual) matches the oracle's direct solve
-        assert M.solve(nsteps=1, tol=1e-11, lin_rtol=1e-12).converged
+        # near-exact inner solves, so the displacement itself (not only the
+        # residual) matches the oracle's direct solve; 1e-10 stays above the
+        # FP64 residual floor of this slender beam (about 6e-12 relative)
+        assert M.solve(nsteps=1, tol=1e-10, lin_rtol=1e-12).converged
         return M, mesh
 
     M20, _ = tip(20)
@@ -74,7 +75,7 @@ def test_T14_cantilever_vs_beam_theory_and_oracle(oracle):
     om = oracle.OracleModel(mesh40.nodes, mesh40.elements, oracle.J2Material(E, NU, 1e9), small=True)
     om.fix(P.on_face(mesh40, "xmin"), "all")
     om.load(P.on_face(mesh40, "xmax"), "z", -Pz, distribute=True)
-    assert om.solve(nsteps=1, tol=1e-12)["converged"]
+    assert om.solve(nsteps=1, tol=1e-10)["converged"]
     assert np.linalg.norm(M40.U - om.U) / np.linalg.norm(om.U) < 1e-7
 
 
