@@ -168,3 +168,23 @@ def test_bc_builders_match_oracle_loops(oracle):
     n0 = len(M.dir_dofs)
     M.fix([1], "z")
     assert len(M.dir_dofs) == n0 + 1 and M.dir_dofs[-1] == 3 and M._bcs_dirty
+
+
+def test_abi_structs_match_header():
+    """The ctypes mirrors of pfem_material, pfem_solve_opts and pfem_solve_result
+    list the header's fields in order with the same C types (the library writes
+    through these structs, so a mismatch would corrupt memory)."""
+    hdr = open(os.path.join(ROOT, "include", "pfem_b200.h")).read()
+    ctype = {"int32_t": C.c_int32, "double": C.c_double, "int64_t": C.c_int64}
+    for cname, pycls in (("pfem_material", L.Material), ("pfem_solve_opts", L.SolveOpts),
+                         ("pfem_solve_result", L.SolveResultC)):
+        body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (cname, cname), hdr, re.S).group(1)
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            t, names = decl.split(None, 1)
+            fields += [(n.strip(), ctype[t]) for n in names.split(",")]
+        assert [(n, t) for n, t in pycls._fields_] == fields, cname
