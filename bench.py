@@ -187,18 +187,9 @@ def main():
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as td
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=timedelta(seconds=600),
-                              device_id=torch.device("cuda", local))
-        dist = td
+    from plasticity_b200.replicas import Replicas
+    reps = Replicas("nccl")
+    rank, world, local = reps.rank, reps.world, reps.local
 
     from plasticity_b200 import workloads as W
     w = W.config2(n=args.n)
@@ -237,17 +228,8 @@ def main():
             PR.load_into(M)
         return M
 
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = reps.barrier
+    max_over_ranks = reps.max_over_ranks
 
     from plasticity_b200 import _lib as L
 
@@ -394,9 +376,7 @@ def main():
                 "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": gpu_launches, **out_extra}
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
 
 
 if __name__ == "__main__":
