@@ -1,6 +1,6 @@
 """GPU parity of the CUDA path against the CPU oracle and its golden fixtures.
 
-Bars (north_star): CSR pattern, colors and per-Gauss-point elastic/plastic flags
+Bars: CSR pattern, colors and per-Gauss-point elastic/plastic flags
 bit-exact; converged displacements within 1e-8 relative; Cauchy stress and
 equivalent plastic strain within 1e-6 relative; Newton iterations within +-1.
 Element-level quantities use tighter FP64 bars (1e-9 normwise) and 1e-6 for the

@@ -36,7 +36,7 @@ def test_T1_elastic_roundtrip(oracle):
 
 @pytest.mark.parametrize("exx", [0.004, 0.007, 0.01])
 def test_T2_uniaxial_closed_form(oracle, exx):
-    # test_material.jl:23-52; 258.77 MPa at exx = 0.01 (docs/DESIGN.md T2)
+    # test_material.jl:23-52; 258.77 MPa at exx = 0.01, the reference's own T2 value
     mat = oracle.J2Material(E, NU, SY, HI)
     s = _uniaxial(oracle, mat, exx)
     Ht = E * HI / (E + HI)
