@@ -162,3 +162,18 @@ def test_saturation_solve_vs_oracle(oracle, kind):
     if kind == "small":
         m = P.J2Material(**mat)
         assert sig[:, 0].mean() == pytest.approx(m.yield_stress(a.mean()), rel=1e-6)
+
+
+def test_back_stress_set_get_roundtrip():
+    # pfem_set_back_stress / pfem_get_back_stress (GaussState.beta, Mesh.jl:124-130)
+    mesh = P.box_mesh(1.0, 1.0, 1.0, 2, 2, 2)
+    M = P.Model(mesh, P.J2Material(**MATS["kin"]), element="finite")
+    b = np.random.default_rng(2).standard_normal((M.ngp, 6))
+    M.set_back_stress(b)
+    assert np.array_equal(M.back_stress(), b)
+    M.reset()
+    assert not M.back_stress().any()
+    L_ = P.Model(mesh, P.J2Material(**MATS["voce"]), element="finite")
+    assert not L_.back_stress().any()
+    with pytest.raises(P.PfemError):
+        L_.set_back_stress(b)
