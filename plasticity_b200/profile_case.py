@@ -11,7 +11,9 @@ default), sets a displacement that drives most Gauss points plastic (uniform
      (weights from plasticity_b200/weights when present, else random),
   5. two AMG set-ups and `reps` AMG-preconditioned CG solves (relative
      tolerance 1e-4, the device-side CG graph) on the imposed mixed-precision
-     tangent at that displacement.
+     tangent at that displacement,
+  6. `reps` single applications of the preconditioner (one V-cycle on level 0,
+     W below) outside the graph, so a launch list shows its kernels one by one.
 
 Each family is timed with CUDA events on the library's stream and printed as one
 JSON line, so the same command serves a launch list, a single-kernel capture
@@ -73,6 +75,11 @@ def main():
     for _ in range(args.reps):
         M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed")
     out["cg_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    M.amg_apply(-R)
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        M.amg_apply(-R)
+    out["amg_cycle_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
     print(json.dumps(out), flush=True)
 
 
