@@ -2,6 +2,9 @@
 // Dirichlet imposition and AMG transfer kernels.  All are HBM-bound; each is
 // written so that one pass over the matrix does all the work the caller needs
 // from that pass (SpMV + residual, SpMV + block-Jacobi Chebyshev update).
+#include <cstdint>
+#include <type_traits>
+
 #include "linalg.cuh"
 
 namespace pfem {
@@ -13,7 +16,7 @@ namespace pfem {
 //   0: y = A x
 //   1: y = b - A x                          (residual)
 //   2: r -= Dinv (A x); xo += x             (Chebyshev step on x = d)
-template <typename T, int BS, int MODE>
+template <typename T, int BS, int MODE, bool VEC = false>
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __restrict__ rowptr,
                                                        const int* __restrict__ col,
                                                        const T* __restrict__ val,
@@ -35,8 +38,24 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
     const int c = __ldcs(col + k);
     const T* B = val + (long long)k * (BS * BS);
     T bv[BS * BS];
+    if constexpr (VEC) {
+      // 16-byte streaming loads (a 6 x 6 block is 144 / 288 bytes; the launcher
+      // checks that val is 16-byte aligned, so every block is)
+      using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
+      constexpr int PER = 16 / (int)sizeof(T), NV = BS * BS / PER;
+      static_assert(BS * BS % PER == 0, "vector loads need whole 16-byte groups");
+      const V* B4 = reinterpret_cast<const V*>(B);
 #pragma unroll
-    for (int q = 0; q < BS * BS; ++q) bv[q] = __ldcs(B + q);
+      for (int q = 0; q < NV; ++q) {
+        const V v = __ldcs(B4 + q);
+        const T* vt = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) bv[q * PER + j] = vt[j];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < BS * BS; ++q) bv[q] = __ldcs(B + q);
+    }
     T xv[BS];
 #pragma unroll
     for (int j = 0; j < BS; ++j) xv[j] = x[(long long)c * BS + j];
@@ -100,6 +119,9 @@ static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const 
   pfem::count_launch();
   if (A.bs == 3)
     bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+  else if ((reinterpret_cast<uintptr_t>(A.val) & 15) == 0)
+    bsr_spmv_kernel<T, 6, MODE, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1,
+                                                              c2);
   else
     bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
 }
