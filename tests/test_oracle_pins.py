@@ -302,3 +302,63 @@ def test_small_strain_element_fd_tangent_and_symmetry(oracle):
                      - oracle.element(2, mat, Xe, ue - e, cpi=epsp, alpha=alpha)["Fe"]) / (2 * h)
     assert np.abs(K - Kfd).max() <= 1e-6 * np.abs(K).max()
     assert np.abs(K - K.T).max() <= 1e-10 * np.abs(K).max()
+
+
+# ---- remaining finite-strain system tests (test_finite_strain.jl:97-113, :158-168, :270-300) ----
+def _fs_uniaxial(O, small, disp, nx=2, nsteps=5, mat=None):
+    import plasticity_b200 as P
+    mesh = P.box_mesh(1.0, 1.0, 1.0, nx, nx, nx)
+    m = mat or O.J2Material(E, NU, SY, HI)
+    om = O.OracleModel(mesh.nodes, mesh.elements, m, fbar=False, small=small)
+    om.fix(P.on_face(mesh, "xmin"), "x"); om.fix(P.on_face(mesh, "ymin"), "y"); om.fix(P.on_face(mesh, "zmin"), "z")
+    om.prescribe(P.on_face(mesh, "xmax"), "x", disp)
+    res = om.solve(nsteps=nsteps, tol=1e-10)
+    return om, res
+
+
+def test_F1_small_displacement_limit(oracle):
+    for disp in (1e-6, 1e-5, 1e-4):
+        ms, _ = _fs_uniaxial(oracle, True, disp)
+        mf, _ = _fs_uniaxial(oracle, False, disp)
+        assert np.linalg.norm(mf.U - ms.U) / np.linalg.norm(ms.U) < 0.5 * disp + 1e-9
+    ms, _ = _fs_uniaxial(oracle, True, 1e-6)
+    mf, _ = _fs_uniaxial(oracle, False, 1e-6)
+    assert np.linalg.norm(mf.U - ms.U) / np.linalg.norm(ms.U) < 1e-6
+
+
+def test_F2prime_newton_quadratic_finite(oracle):
+    _, res = _fs_uniaxial(oracle, False, 0.05, nsteps=3)
+    assert res["converged"]
+    r = res["residuals"][-1]
+    assert len(r) <= 6
+    if len(r) >= 4:
+        assert r[-1] < r[-2] ** 1.5 + 1e-12
+
+
+def _bend(O, fbar, small=False):
+    import plasticity_b200 as P
+    mesh = P.box_mesh(6.0, 1.0, 1.0, 6, 2, 2)
+    om = O.OracleModel(mesh.nodes, mesh.elements, O.J2Material(E, 0.49, SY, 500.0), fbar=fbar, small=small)
+    om.fix(P.on_face(mesh, "xmin"), "all")
+    om.load(P.on_face(mesh, "xmax"), "z", -10.0, distribute=True)
+    res = om.solve(nsteps=6, tol=1e-7, maxiter=40)
+    return res["converged"], np.abs(om.U.reshape(-1, 3)[:, 2]).max()
+
+
+def test_F6_F7_fbar_relieves_volumetric_locking(oracle):
+    cf, df = _bend(oracle, True)
+    cs, ds = _bend(oracle, False)
+    assert cf and cs
+    assert df > 1.3 * ds
+
+
+def test_F8_large_rotation_cantilever(oracle):
+    import plasticity_b200 as P
+    mesh = P.box_mesh(8.0, 1.0, 1.0, 8, 1, 1)
+    om = oracle.OracleModel(mesh.nodes, mesh.elements, oracle.J2Material(E, NU, 1e9), fbar=False)
+    om.fix(P.on_face(mesh, "xmin"), "all")
+    om.load(P.on_face(mesh, "xmax"), "z", -300.0, distribute=True)
+    res = om.solve(nsteps=6, tol=1e-8, maxiter=40)
+    assert res["converged"]
+    assert np.abs(om.U.reshape(-1, 3)[:, 2]).max() > 0.1
+    assert np.all(np.isfinite(om.U))
