@@ -218,6 +218,58 @@ def pattern(nn, elems):
     return colptr, rowval
 
 
+def box_nd_dofs(nx, ny, nz, leaf=64):
+    """A nested-dissection order of the dofs of an (nx+1)(ny+1)(nz+1)-node box grid
+    numbered i fastest (box_mesh, Mesh.jl:30-59): split the longest index range at
+    its middle plane, order both halves recursively, the separator plane last.
+    Any fill-reducing order leaves an exact LU's solution unchanged to rounding; this
+    one keeps SuperLU's fill near the nested-dissection bound on box meshes, where its
+    own orderings (COLAMD, MMD) fill 2-4x more."""
+    npx, npy = nx + 1, ny + 1
+    out = []
+
+    def rec(i0, i1, j0, j1, k0, k1):
+        di, dj, dk = i1 - i0, j1 - j0, k1 - k0
+        if di <= 0 or dj <= 0 or dk <= 0:
+            return
+        if di * dj * dk <= leaf or max(di, dj, dk) < 3:
+            k, j, i = np.meshgrid(np.arange(k0, k1), np.arange(j0, j1), np.arange(i0, i1), indexing="ij")
+            out.append(((k * npy + j) * npx + i).ravel())
+            return
+        if di >= dj and di >= dk:
+            m = (i0 + i1) // 2
+            rec(i0, m, j0, j1, k0, k1); rec(m + 1, i1, j0, j1, k0, k1); rec(m, m + 1, j0, j1, k0, k1)
+        elif dj >= dk:
+            m = (j0 + j1) // 2
+            rec(i0, i1, j0, m, k0, k1); rec(i0, i1, m + 1, j1, k0, k1); rec(i0, i1, m, m + 1, k0, k1)
+        else:
+            m = (k0 + k1) // 2
+            rec(i0, i1, j0, j1, k0, m); rec(i0, i1, j0, j1, m + 1, k1); rec(i0, i1, j0, j1, m, m + 1)
+
+    rec(0, nx + 1, 0, ny + 1, 0, nz + 1)
+    pn = np.concatenate(out)
+    return (3 * pn[:, None] + np.arange(3)[None, :]).ravel()
+
+
+def nd_lu_solver(perm, stats=None):
+    """linsolve(K, b) for OracleModel.newton: sparse LU (SuperLU, standing in for
+    the reference's UMFPACK, Solver.jl:237-240) of K in the symmetric order `perm`.
+    `stats`, a dict, collects the factorisation count and seconds."""
+    import time
+
+    def solve(K, b):
+        t0 = time.perf_counter()
+        Kp = K.tocsc()[perm][:, perm].tocsc()
+        lu = spla.splu(Kp, permc_spec="NATURAL", diag_pivot_thresh=0.01, options=dict(SymmetricMode=True))
+        x = np.empty_like(b)
+        x[perm] = lu.solve(b[perm])
+        if stats is not None:
+            stats["lu"] = stats.get("lu", 0) + 1
+            stats["lu_s"] = stats.get("lu_s", 0.0) + time.perf_counter() - t0
+        return x
+    return solve
+
+
 def element_colors(nodes, elems):
     """element_colors (Assembly.jl:172-206) as a 0-based color id per element."""
     nn, ne = nodes.shape[1], elems.shape[1]

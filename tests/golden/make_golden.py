@@ -66,8 +66,48 @@ def solve_case(w, fname, line_search=False):
           float(out["flags"].mean()))
 
 
+def solve_prefix_case(w, dims, last, fname, line_search=False):
+    """The first `last` increments of a load path at a size where the LU needs a
+    fill-reducing order: Newton counts at the case tolerance, U (FP64), Cauchy
+    stress and alpha (FP32: the bars are 1e-6 relative to their maxima, FP32
+    rounding is 6e-8 of each value) and flags (bit-packed) at 1e-12 after
+    increment `last`."""
+    mat = O.J2Material(**{k: w.material[k] for k in ("E", "nu", "sigy0", "Hiso", "Hkin")})
+    perm = O.box_nd_dofs(*dims)
+    out = {}
+    for tol in (w.tol, 1e-12):
+        m = O.OracleModel(w.mesh.nodes, w.mesh.elements, mat, fbar=True, sigy0_e=w.sigy0_e, nthreads=0)
+        w.apply(m)
+        ramp, fix = m.freeze_bcs()
+        its = []
+        for s in range(1, last + 1):
+            conv, hist = m.newton(s / w.nsteps, ramp, fix, tol, 25, linsolve=O.nd_lu_solver(perm),
+                                  line_search=line_search)
+            assert conv, (fname, tol, s, hist)
+            _, _, m.tau, m.flags = m.assemble(m.U, commit=True)
+            its.append(len(hist))
+            print(fname, tol, s, len(hist), flush=True)
+        if tol == w.tol:
+            out["iters"] = np.array(its)
+        else:
+            out.update(U=m.U, sigma=m.gauss_stress().astype(np.float32), alpha=m.alpha.astype(np.float32),
+                       flags_bits=np.packbits(m.flags), ngp=len(m.flags), iters_tight=np.array(its))
+    np.savez_compressed(os.path.join(HERE, fname), nsteps=w.nsteps, last=last, tol=w.tol,
+                        line_search=int(line_search), **out)
+    print(fname, list(out["iters"]), float(np.abs(out["U"]).max()), float(out["alpha"].max()))
+
+
+CASES = {
+    "element": element_cases,
+    "config0": lambda: solve_case(W.config0(n=8), "config0_cube8.npz"),
+    "cube4": lambda: solve_case(W.config2(n=4, nsteps=40), "cube4_jitter_compress.npz", line_search=True),
+    "bar8": lambda: solve_case(W.config1(nx=8, ny=2, nz=2, nsteps=6, stretch=0.05), "bar8x2x2_neck.npz"),
+    # configuration 1 at its stated size (80x16x16, 70,227 DOF), first 15 of its 60 increments
+    "bar80": lambda: solve_prefix_case(W.config1(), (80, 16, 16), 15, "bar80x16x16_neck_15.npz"),
+    # configuration 2's workload at 16^3 (14,739 DOF), the whole 40-increment path
+    "cube16": lambda: solve_prefix_case(W.config2(n=16), (16, 16, 16), 40, "cube16_jitter_compress.npz"),
+}
+
 if __name__ == "__main__":
-    element_cases()
-    solve_case(W.config0(n=8), "config0_cube8.npz")
-    solve_case(W.config2(n=4, nsteps=40), "cube4_jitter_compress.npz", line_search=True)
-    solve_case(W.config1(nx=8, ny=2, nz=2, nsteps=6, stretch=0.05), "bar8x2x2_neck.npz")
+    for name in (sys.argv[1:] or list(CASES)):
+        CASES[name]()
