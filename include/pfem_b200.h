@@ -2,8 +2,9 @@
  * pfem_b200.h -- C ABI of the B200 finite-strain F-bar J2 plasticity path.
  *
  * Drop-in for the per-Newton-iteration path of vinaysrao1/plasticity,
- * lagrangian/ (Julia).  A Julia shim binds these symbols with `ccall` (see
- * INTEGRATION.md); the Python package `plasticity_b200` binds them with ctypes.
+ * lagrangian/ (Julia).  A Julia shim binds these symbols with `ccall`, passing
+ * its own arrays (GC.@preserve'd for the call); the Python package
+ * `plasticity_b200` binds them with ctypes.
  *
  * Conventions (same as the reference):
  *   - node coordinates: 3 x nn, column-major (nodes[3*n + d]), Mesh.jl:17-22

@@ -92,8 +92,15 @@ extern "C" int pfem_norm2_noalloc(const double* x, int64_t n, double* result, vo
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) {
+  if (e != cudaSuccess) {
     pfem::set_last_error(std::string("pfem_norm2_noalloc: no usable current device: ") + cudaGetErrorString(e));
+    return PFEM_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= NA_MAX_DEVICES) {
+    char buf[160];
+    snprintf(buf, sizeof(buf), "pfem_norm2_noalloc: current device index %d is outside the %d devices supported",
+             dev, NA_MAX_DEVICES);
+    pfem::set_last_error(buf);
     return PFEM_ERR_CUDA;
   }
   double* part = nullptr;
