@@ -110,6 +110,7 @@ struct pfem_ctx {
   double *dUtmp = nullptr, *dScal = nullptr, *dPart = nullptr;
   double* dK64 = nullptr;
   float* dK32 = nullptr;
+  double* dDenseWork = nullptr;  // FP64 work matrix of the coarse dense inverse (both precisions)
   DevStatus* dStatus = nullptr;
   // boundary conditions
   bool bcs_set = false;
@@ -179,6 +180,22 @@ cudaError_t upload(pfem_ctx* ctx, T** p, const std::vector<T>& h) {
 }
 
 // Free one allocation made by dalloc/upload (nullptr is a no-op).
+// Device temporaries of one entry-point call, released on every return path
+// (including the early returns of CK).
+struct TmpDev {
+  std::vector<void*> p;
+  template <typename T>
+  cudaError_t alloc(T** out, size_t bytes) {
+    *out = nullptr;
+    cudaError_t e = cudaMalloc((void**)out, bytes);
+    if (e == cudaSuccess) p.push_back((void*)*out);
+    return e;
+  }
+  ~TmpDev() {
+    for (void* q : p) cudaFree(q);
+  }
+};
+
 template <typename T>
 void dfree(pfem_ctx* ctx, T*& p) {
   if (!p) return;
@@ -418,6 +435,12 @@ void mgs_qr(int m, std::vector<double>& A, double R[36]) {
 // (Solver.jl:117-129), and the patterns of P = (I - w D^-1 A) T, of A P and
 // of the Galerkin operator P^T A P of every level.  Level 0 uses the
 // tangent's block pattern in place (its rowptr/col stay empty).
+// The hierarchy stops at the first level with at most this many unknowns; that
+// level is inverted densely on the device (dense.cu) and applied as one dense
+// matrix-vector product per cycle.  At 64^3 this is level 2 (512 aggregates,
+// 3,072 unknowns): one product in place of a W-cycle's two visits to it.
+constexpr long long kCoarseDenseMax = 3600;
+
 void build_amg_structure(pfem_ctx* c) {
   c->hl.clear();
   HostLevel cur;
@@ -430,7 +453,7 @@ void build_amg_structure(pfem_ctx* c) {
   bool first = true;
   for (int lev = 0; lev < 10; ++lev) {
     const int nb = cur.nbrow, bs = cur.bs;
-    if ((long long)nb * bs <= 600 && !first) break;
+    if ((long long)nb * bs <= kCoarseDenseMax && !first) break;
     const int* rp = first ? c->browptr.data() : cur.rowptr.data();
     const int* cl = first ? c->bcol.data() : cur.col.data();
     const int* grp = first ? rp : cur.grp.data();
@@ -623,7 +646,13 @@ int amg_alloc(pfem_ctx* ctx) {
     v.nnzP = (int)h.p_cl.size();
     CK(upload(ctx, &v.p_rp, h.p_rp)); CK(upload(ctx, &v.p_cl, h.p_cl)); CK(upload(ctx, &v.p_row, h.p_row));
     CK(upload(ctx, &v.pslot, h.pslot)); CK(upload(ctx, &v.pt_rp, h.pt_rp)); CK(upload(ctx, &v.pt_blk, h.pt_blk));
+    {
+      std::vector<int> ptr_row(h.pt_blk.size());
+      for (size_t t = 0; t < h.pt_blk.size(); ++t) ptr_row[t] = h.p_row[h.pt_blk[t]];
+      CK(upload(ctx, &v.pt_row, ptr_row));
+    }
     CK(dalloc(ctx, &v.p_val, (size_t)v.nnzP * h.bs * 6));
+    CK(dalloc(ctx, &v.pt_val, (size_t)v.nnzP * h.bs * 6));
     v.nnzAP = (int)h.ap_cl.size();
     CK(upload(ctx, &v.ap_rp, h.ap_rp)); CK(upload(ctx, &v.ap_cl, h.ap_cl)); CK(upload(ctx, &v.ap_row, h.ap_row));
     CK(dalloc(ctx, &v.ap_val, (size_t)v.nnzAP * h.bs * 6));
@@ -637,7 +666,10 @@ int amg_alloc(pfem_ctx* ctx) {
   A.coarse_n = hc.nbrow * hc.bs;
   A.coarse_nnzb = hc.rowptr[hc.nbrow];
   CK(dalloc(ctx, &A.coarse_val, (size_t)A.coarse_nnzb * 36));
+  CK(upload(ctx, &A.coarse_rp, hc.rowptr));
+  CK(upload(ctx, &A.coarse_cl, hc.col));
   CK(dalloc(ctx, &A.coarse_inv, (size_t)A.coarse_n * A.coarse_n));
+  if (!ctx->dDenseWork) CK(dalloc(ctx, &ctx->dDenseWork, (size_t)pfem::dense_inverse_work_doubles(A.coarse_n)));
   CK(dalloc(ctx, &A.cx, (size_t)A.coarse_n));
   CK(dalloc(ctx, &A.cb, (size_t)A.coarse_n));
   return PFEM_OK;
@@ -654,46 +686,13 @@ int krylov_alloc(pfem_ctx* ctx) {
   CK(dalloc(ctx, &w.v, n)); CK(dalloc(ctx, &w.s, n)); CK(dalloc(ctx, &w.t, n));
   CK(dalloc(ctx, &w.ph, n)); CK(dalloc(ctx, &w.sh, n)); CK(dalloc(ctx, &w.b, n));
   CK(dalloc(ctx, &w.xa, n)); CK(dalloc(ctx, &w.b0, n));
-  CK(dalloc(ctx, &w.sc, 16)); CK(dalloc(ctx, &w.part, 2048));
+  CK(dalloc(ctx, &w.sc, 16)); CK(dalloc(ctx, &w.part, 3 * 2048));  // three partial sets of the fused PCG body
   return PFEM_OK;
-}
-
-// Gauss-Jordan inverse of a dense n x n matrix (row-major, double) with
-// partial pivoting; near-singular pivots are regularised.
-void dense_inverse(int n, std::vector<double>& a, std::vector<double>& inv) {
-  inv.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
-  double scl = 0;
-  for (int i = 0; i < n; ++i) scl = std::max(scl, std::fabs(a[(size_t)i * n + i]));
-  for (int c = 0; c < n; ++c) {
-    int piv = c;
-    double best = std::fabs(a[(size_t)c * n + c]);
-    for (int r = c + 1; r < n; ++r)
-      if (std::fabs(a[(size_t)r * n + c]) > best) { best = std::fabs(a[(size_t)r * n + c]); piv = r; }
-    if (piv != c)
-      for (int j = 0; j < n; ++j) {
-        std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
-        std::swap(inv[(size_t)c * n + j], inv[(size_t)piv * n + j]);
-      }
-    double pv = a[(size_t)c * n + c];
-    if (std::fabs(pv) < 1e-14 * std::max(scl, 1e-300)) pv = (pv >= 0 ? 1.0 : -1.0) * 1e-14 * std::max(scl, 1e-300);
-    const double ip = 1.0 / pv;
-    for (int j = 0; j < n; ++j) { a[(size_t)c * n + j] *= ip; inv[(size_t)c * n + j] *= ip; }
-    for (int r = 0; r < n; ++r) {
-      if (r == c) continue;
-      const double f = a[(size_t)r * n + c];
-      if (f == 0.0) continue;
-      for (int j = 0; j < n; ++j) {
-        a[(size_t)r * n + j] -= f * a[(size_t)c * n + j];
-        inv[(size_t)r * n + j] -= f * inv[(size_t)c * n + j];
-      }
-    }
-  }
 }
 
 // Numeric AMG set-up on the current (Dirichlet-imposed) tangent of precision T:
 // block-Jacobi inverses, Chebyshev bounds by power iteration, Galerkin
-// coarse operators, dense coarse inverse.  Rebuilt per load step by default
+// coarse operators, dense coarse inverse -- all on the device.  Rebuilt per load step by default
 // (the reference's reuse policy, Solver.jl:243-245).
 template <typename T>
 int amg_setup(pfem_ctx* ctx, int cheb_degree) {
@@ -736,31 +735,10 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     sa_setup_level<T>(v, omega, cval, nnzC, ctx->st);
     CKL();
   }
-  // coarsest operator: dense inverse on the host (a few hundred dofs)
-  {
-    const HostLevel& hc = ctx->hl[L];
-    std::vector<T> hv((size_t)A.coarse_nnzb * 36);
-    CK(cudaMemcpyAsync(hv.data(), A.coarse_val, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    const int n = A.coarse_n;
-    std::vector<double> dense((size_t)n * n, 0.0), inv;
-    for (int I = 0; I < hc.nbrow; ++I)
-      for (int k = hc.rowptr[I]; k < hc.rowptr[I + 1]; ++k) {
-        const int J = hc.col[k];
-        for (int r = 0; r < 6; ++r)
-          for (int c = 0; c < 6; ++c) dense[(size_t)(I * 6 + r) * n + J * 6 + c] = (double)hv[(size_t)k * 36 + r * 6 + c];
-      }
-    // rigid modes absent from an aggregate leave zero rows: put 1 on their diagonal
-    for (int i = 0; i < n; ++i) {
-      bool zero = true;
-      for (int j = 0; j < n && zero; ++j) zero = dense[(size_t)i * n + j] == 0.0;
-      if (zero) dense[(size_t)i * n + i] = 1.0;
-    }
-    dense_inverse(n, dense, inv);
-    std::vector<T> invT(inv.begin(), inv.end());
-    CK(cudaMemcpyAsync(A.coarse_inv, invT.data(), invT.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-  }
+  // coarsest operator: dense inverse on the device (at most kCoarseDenseMax unknowns)
+  pfem::dense_coarse_inverse<T>(ctx->hl[L].nbrow, A.coarse_rp, A.coarse_cl, A.coarse_val, A.coarse_n,
+                                ctx->dDenseWork, A.coarse_inv, ctx->st);
+  CKL();
   A.built = true;
   A.version++;
   return PFEM_OK;
@@ -841,12 +819,29 @@ __global__ void cg_graph_init_kernel(cudaGraphConditionalHandle h, const T* __re
   *sc0 = T(1);                  // with p = 0, the first update p = z + (r.z / 1) p gives p = z
   cudaGraphSetConditional(h, (b > 0.0 && isfinite(b)) ? 1u : 0u);
 }
+// End of a PCG iteration: |r| from the np partials of r.r (fixed order, one
+// CTA of 1024 threads), into sc_rn, then the loop condition.
 template <typename T>
-__global__ void cg_graph_check_kernel(cudaGraphConditionalHandle h, const T* __restrict__ rn,
-                                      const double* __restrict__ ctl, int* __restrict__ state) {
+__global__ void cg_graph_check_kernel(cudaGraphConditionalHandle h, const T* __restrict__ part, int np,
+                                      T* __restrict__ sc_rn, const double* __restrict__ ctl,
+                                      int* __restrict__ state) {
+  __shared__ T sh[32];
+  T v = T(0);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : T(0);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (threadIdx.x != 0) return;
+  const T rn = sqrt(v);
+  *sc_rn = rn;
   const int it = state[0] + 1;
   state[0] = it;
-  const double r = (double)*rn;
+  const double r = (double)rn;
   const bool conv = r <= ctl[2];
   state[1] = conv ? 1 : 0;
   cudaGraphSetConditional(h, (!conv && isfinite(r) && it < (int)ctl[1]) ? 1u : 0u);
@@ -918,14 +913,17 @@ int cg_graph_build(pfem_ctx* ctx) {
   ctx->st = bs;  // the V-cycle launches on ctx->st
   vcycle<T>(ctx, 0, w.r, w.z);
   ctx->st = st;
-  dot<T>(n, w.r, w.z, w.sc + 2, w.part, bs, false);
-  cg_p<T>(n, w.sc + 2, w.sc + 0, w.z, w.p, bs);
-  scalar_copy<T>(w.sc + 0, w.sc + 2, bs);
+  // sc[0] = r.z of the previous iteration, sc[2] = r.z; the final sums of the
+  // three dot products happen inside the kernels that use them
+  T* const part_rz = w.part;
+  T* const part_pq = w.part + 2048;
+  T* const part_rr = w.part + 4096;
+  const int np_rz = dot_partials<T>(n, w.r, w.z, part_rz, bs);
+  cg_p_fused<T>(n, part_rz, np_rz, w.sc, w.z, w.p, bs);
   bsr_spmv<T>(K, w.p, w.q, bs);
-  dot<T>(n, w.p, w.q, w.sc + 1, w.part, bs, false);
-  cg_xr<T>(n, w.sc + 0, w.sc + 1, w.p, w.q, w.x, w.r, bs);
-  dot<T>(n, w.r, w.r, w.sc + 3, w.part, bs, true);
-  cg_graph_check_kernel<T><<<1, 1, 0, bs>>>(h, w.sc + 3, G.ctl, G.state);
+  const int np_pq = dot_partials<T>(n, w.p, w.q, part_pq, bs);
+  const int np_rr = cg_xr_fused<T>(n, part_pq, np_pq, w.sc, w.p, w.q, w.x, w.r, part_rr, bs);
+  cg_graph_check_kernel<T><<<1, 1024, 0, bs>>>(h, part_rr, np_rr, w.sc + 3, G.ctl, G.state);
   e = cudaStreamEndCapture(bs, &body);
   if (e != cudaSuccess) return abort_capture(e, "body end");
   const long long c2 = pfem::launch_counter();
@@ -1811,10 +1809,14 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   BcDev& b = ctx->bc;
   if (ctx->bcs_set && dofs == ctx->bc_dofs) {
     // same constrained dofs: the imposition lists stand, only values change
+    // not usable until every copy has landed: a failed copy leaves the context
+    // without boundary conditions rather than with a half-updated set
+    ctx->bcs_set = false;
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaMemcpy(b.vals, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b.ramp, ramp.data(), ramp.size() * sizeof(uint8_t), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b.fn, fn.data(), fn.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->bcs_set = true;
     return PFEM_OK;
   }
   // entries touched by the imposition
@@ -1858,6 +1860,11 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   rptr.push_back((int)rpos.size());
   if (rows.empty()) rptr.assign(1, 0);
   for (auto& z : zl) { zpos.push_back(z.first); zone.push_back(z.second); }
+  // the old lists go away before the new ones exist: until every upload below has
+  // succeeded the context has no boundary conditions (a later call with the same
+  // dofs must take this path again, not the value-only fast path above)
+  ctx->bcs_set = false;
+  ctx->bc_dofs.clear();
   dfree(ctx, b.dofs); dfree(ctx, b.vals); dfree(ctx, b.ramp); dfree(ctx, b.fn); dfree(ctx, b.rows);
   dfree(ctx, b.rptr); dfree(ctx, b.rpos); dfree(ctx, b.rcol); dfree(ctx, b.zpos); dfree(ctx, b.zone);
   b = BcDev();
@@ -2530,16 +2537,16 @@ int pfem_mlp_forward(pfem_ctx* ctx, const float* feats, int64_t n, float* out) {
   int rc = mlp_alloc(ctx);
   if (rc) return rc;
   float *df = nullptr, *dy = nullptr;
-  void* db = nullptr;
-  CK(cudaMalloc((void**)&df, (size_t)n * MLP_NFEAT * sizeof(float)));
-  CK(cudaMalloc(&db, (size_t)n * 32));
-  CK(cudaMalloc((void**)&dy, (size_t)n * 3 * sizeof(float)));
+  char* db = nullptr;
+  TmpDev tmp;
+  CK(tmp.alloc(&df, (size_t)n * MLP_NFEAT * sizeof(float)));
+  CK(tmp.alloc(&db, (size_t)n * 32));
+  CK(tmp.alloc(&dy, (size_t)n * 3 * sizeof(float)));
   CK(cudaMemcpy(df, feats, (size_t)n * MLP_NFEAT * sizeof(float), cudaMemcpyHostToDevice));
   mlp_pack_features(df, n, db, ctx->st);
   rc = mlp_launch(false, ctx->mlp.w, db, nullptr, nullptr, n, dy, nullptr, nullptr, ctx->mlp.err, 148, ctx->st);
   CK(cudaStreamSynchronize(ctx->st));
   CK(cudaMemcpy(out, dy, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost));
-  cudaFree(df); cudaFree(db); cudaFree(dy);
   if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
   return mlp_check_err(ctx);
 }
@@ -2551,10 +2558,11 @@ int pfem_mlp_loss_grad(pfem_ctx* ctx, const float* feats, const float* targets, 
   int rc = mlp_alloc(ctx);
   if (rc) return rc;
   float *df = nullptr, *dt = nullptr;
-  void* db = nullptr;
-  CK(cudaMalloc((void**)&df, (size_t)n * MLP_NFEAT * sizeof(float)));
-  CK(cudaMalloc(&db, (size_t)n * 32));
-  CK(cudaMalloc((void**)&dt, (size_t)n * 3 * sizeof(float)));
+  char* db = nullptr;
+  TmpDev tmp;
+  CK(tmp.alloc(&df, (size_t)n * MLP_NFEAT * sizeof(float)));
+  CK(tmp.alloc(&db, (size_t)n * 32));
+  CK(tmp.alloc(&dt, (size_t)n * 3 * sizeof(float)));
   CK(cudaMemcpy(df, feats, (size_t)n * MLP_NFEAT * sizeof(float), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dt, targets, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice));
   mlp_pack_features(df, n, db, ctx->st);
@@ -2567,7 +2575,6 @@ int pfem_mlp_loss_grad(pfem_ctx* ctx, const float* feats, const float* targets, 
   float l = 0;
   CK(cudaMemcpy(&l, ctx->mlp.loss, sizeof(float), cudaMemcpyDeviceToHost));
   if (loss) *loss = l / (3.0f * (float)n);
-  cudaFree(df); cudaFree(db); cudaFree(dt);
   if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
   return mlp_check_err(ctx);
 }
@@ -2610,7 +2617,8 @@ int pfem_mlp_train(pfem_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64
     m.rows_cap = batch;
   }
   float* dl = nullptr;
-  CK(cudaMalloc((void**)&dl, (size_t)steps * sizeof(float)));
+  TmpDev tmp;
+  CK(tmp.alloc(&dl, (size_t)steps * sizeof(float)));
   int rc = 0;
   for (int k = 0; k < steps; ++k) {
     mlp_random_rows(batch, m.ds_n, seed * 1000003ull + (uint64_t)k, m.rows, ctx->st);
@@ -2625,7 +2633,6 @@ int pfem_mlp_train(pfem_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64
     CK(cudaMemcpy(h.data(), dl, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost));
     for (int k = 0; k < steps; ++k) losses[k] = h[k] / (3.0f * (float)batch);
   }
-  cudaFree(dl);
   if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor training kernel launch failed");
   rc = mlp_check_err(ctx);
   if (rc) return rc;

@@ -329,6 +329,75 @@ void cg_p(long long n, const T* num, const T* den, const T* z, T* p, cudaStream_
   const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
   pfem::count_launch(); cg_p_kernel<T><<<blocks, 256, 0, st>>>(n, num, den, z, p);
 }
+// ---- PCG updates with the final reduction fused in ----
+// Every CTA sums the same np partials in the same order (a strided pass and a
+// fixed tree), so all CTAs see the same scalar and the result is deterministic.
+template <typename T>
+__device__ __forceinline__ T all_sum_partials(const T* __restrict__ part, int np, T* sh) {
+  T v = T(0);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  v = block_sum(v, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[32] = v;
+  __syncthreads();
+  return sh[32];
+}
+// rz = sum(part_rz);  p = z + (rz / sc[0]) p;  sc[2] = rz
+template <typename T>
+__global__ void cg_p_fused_kernel(long long n, const T* __restrict__ part, int np, T* __restrict__ sc,
+                                  const T* __restrict__ z, T* __restrict__ p) {
+  __shared__ T sh[33];
+  const T rz = all_sum_partials(part, np, sh);
+  const T be = rz / sc[0];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = z[i] + be * p[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc[2] = rz;
+}
+// pq = sum(part_pq);  alpha = sc[2] / pq;  x += alpha p;  r -= alpha q;
+// part_rr[cta] = this CTA's share of r.r;  sc[0] = sc[2] (r.z of the next beta)
+template <typename T>
+__global__ void cg_xr_fused_kernel(long long n, const T* __restrict__ part_pq, int np, T* __restrict__ sc,
+                                   const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
+                                   T* __restrict__ r, T* __restrict__ part_rr) {
+  __shared__ T sh[33];
+  const T pq = all_sum_partials(part_pq, np, sh);
+  const T al = sc[2] / pq;
+  T acc = T(0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += al * p[i];
+    const T ri = r[i] - al * q[i];
+    r[i] = ri;
+    acc += ri * ri;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) part_rr[blockIdx.x] = acc;
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc[0] = sc[2];
+}
+template <typename T>
+int dot_partials(long long n, const T* a, const T* b, T* part, cudaStream_t st) {
+  long long nb = (n + RED_THREADS - 1) / RED_THREADS;
+  const int blocks = (int)(nb < RED_BLOCKS ? (nb > 0 ? nb : 1) : RED_BLOCKS);
+  pfem::count_launch(); dot_partial_kernel<T><<<blocks, RED_THREADS, 0, st>>>(n, a, b, part);
+  return blocks;
+}
+int fused_update_blocks(long long n) {
+  const long long nb = (n + RED_THREADS - 1) / RED_THREADS;
+  return (int)(nb < RED_BLOCKS ? (nb > 0 ? nb : 1) : RED_BLOCKS);
+}
+template <typename T>
+void cg_p_fused(long long n, const T* part, int np, T* sc, const T* z, T* p, cudaStream_t st) {
+  pfem::count_launch();
+  cg_p_fused_kernel<T><<<fused_update_blocks(n), RED_THREADS, 0, st>>>(n, part, np, sc, z, p);
+}
+template <typename T>
+int cg_xr_fused(long long n, const T* part_pq, int np, T* sc, const T* p, const T* q, T* x, T* r, T* part_rr,
+                cudaStream_t st) {
+  const int blocks = fused_update_blocks(n);
+  pfem::count_launch();
+  cg_xr_fused_kernel<T><<<blocks, RED_THREADS, 0, st>>>(n, part_pq, np, sc, p, q, x, r, part_rr);
+  return blocks;
+}
+
 // BiCGStab helpers with device scalars s[0..]: see krylov code for layout.
 template <typename T>
 __global__ void bicg_p_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ r,
@@ -628,28 +697,37 @@ __global__ void sa_rap_kernel(int nnzC, const int* __restrict__ c_row, const int
     for (int q = 0; q < 6; ++q) O[r * 6 + q] = acc[r][q];
 }
 
-// Restriction bc = P^T r, one warp per aggregate: the lanes stride over the
-// P blocks of the aggregate's column (the fine rows its smoothed basis
-// reaches) and the six partial sums are combined by a fixed xor tree, so the
-// result is deterministic.
+// P^T copy: block t of the aggregate-ordered list is P block pt_blk[t].
 template <typename T, int BS>
-__global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, const int* __restrict__ pt_blk,
-                                   const int* __restrict__ p_row, const T* __restrict__ pval,
-                                   const T* __restrict__ r, T* __restrict__ bc) {
+__global__ void sa_transpose_copy_kernel(int nnzP, const int* __restrict__ pt_blk, const T* __restrict__ pval,
+                                         T* __restrict__ ptval) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)nnzP * BS * 6) return;
+  const long long t = e / (BS * 6);
+  const int q = (int)(e - t * (BS * 6));
+  ptval[e] = pval[(long long)pt_blk[t] * (BS * 6) + q];
+}
+
+// Restriction bc = P^T r, one warp per aggregate: the lanes stride over the
+// aggregate's P blocks in the P^T-ordered copy (consecutive lanes read
+// consecutive blocks) and the six partial sums are combined by a fixed xor
+// tree, so the result is deterministic.
+template <typename T, int BS>
+__global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, const int* __restrict__ pt_row,
+                                   const T* __restrict__ ptval, const T* __restrict__ r, T* __restrict__ bc) {
   const int I = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (I >= nagg) return;  // whole warps exit together
   T s[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
   const int t1 = pt_rp[I + 1];
   for (int t = pt_rp[I] + lane; t < t1; t += 32) {
-    const int p = pt_blk[t];
-    const T* P = pval + (long long)p * BS * 6;
-    const T* rv = r + (long long)p_row[p] * BS;
+    const T* P = ptval + (long long)t * BS * 6;
+    const T* rv = r + (long long)pt_row[t] * BS;
 #pragma unroll
     for (int j = 0; j < BS; ++j) {
       const T rj = rv[j];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) s[c] += __ldcs(P + j * 6 + c) * rj;
+      for (int c = 0; c < 6; ++c) s[c] += __ldg(P + j * 6 + c) * rj;
     }
   }
 #pragma unroll
@@ -692,6 +770,9 @@ void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t s
     pfem::count_launch();
     sa_rap_kernel<T, 3><<<(nnzC + 127) / 128, 128, 0, st>>>(nnzC, v.c_row, v.c_cl, v.pt_rp, v.pt_blk, v.p_row, v.p_val,
                                                            v.ap_rp, v.ap_cl, v.ap_val, cval);
+    pfem::count_launch();
+    sa_transpose_copy_kernel<T, 3><<<(int)(((long long)v.nnzP * 18 + 255) / 256), 256, 0, st>>>(v.nnzP, v.pt_blk,
+                                                                                               v.p_val, v.pt_val);
   } else {
     pfem::count_launch();
     sa_prolongator_kernel<T, 6><<<(v.nnzP + 127) / 128, 128, 0, st>>>(v.nnzP, v.p_row, v.p_cl, v.A.rowptr, v.A.col,
@@ -702,6 +783,9 @@ void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t s
     pfem::count_launch();
     sa_rap_kernel<T, 6><<<(nnzC + 127) / 128, 128, 0, st>>>(nnzC, v.c_row, v.c_cl, v.pt_rp, v.pt_blk, v.p_row, v.p_val,
                                                            v.ap_rp, v.ap_cl, v.ap_val, cval);
+    pfem::count_launch();
+    sa_transpose_copy_kernel<T, 6><<<(int)(((long long)v.nnzP * 36 + 255) / 256), 256, 0, st>>>(v.nnzP, v.pt_blk,
+                                                                                               v.p_val, v.pt_val);
   }
 }
 template <typename T>
@@ -709,8 +793,8 @@ void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st) {
   const long long n = (long long)v.nagg * 32;  // one warp per aggregate
   const int blocks = (int)((n + 255) / 256);
   pfem::count_launch();
-  if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_blk, v.p_row, v.p_val, r, bc);
-  else sa_restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_blk, v.p_row, v.p_val, r, bc);
+  if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
+  else sa_restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
 }
 template <typename T>
 void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
@@ -741,6 +825,10 @@ void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
   template void bicg_xr<T>(long long, const T*, const T*, const T*, const T*, const T*, T*, T*,    \
                            cudaStream_t);                                                          \
   template void scalar_copy<T>(T*, const T*, cudaStream_t);                                        \
+  template int dot_partials<T>(long long, const T*, const T*, T*, cudaStream_t);                   \
+  template void cg_p_fused<T>(long long, const T*, int, T*, const T*, T*, cudaStream_t);           \
+  template int cg_xr_fused<T>(long long, const T*, int, T*, const T*, const T*, T*, T*, T*,         \
+                              cudaStream_t);                                                       \
   template void add_to_double<T>(long long, const T*, double*, cudaStream_t);                      \
   template void impose_dirichlet<T>(const BcDev&, long long, double, const double*, T*, double*,   \
                                     double*, cudaStream_t);                                        \

@@ -43,6 +43,15 @@ template <typename T> void bicg_p(long long n, const T* sc, const T* r, const T*
 template <typename T> void bicg_s(long long n, const T* sc, const T* r, const T* v, T* s, cudaStream_t st);
 template <typename T> void bicg_xr(long long n, const T* sc, const T* ph, const T* sh, const T* s, const T* t, T* x, T* r, cudaStream_t st);
 template <typename T> void scalar_copy(T* dst, const T* src, cudaStream_t st);
+// PCG with the dot products' final sums fused into their consumers (deterministic):
+// dot_partials writes the per-CTA partials of a.b and returns their count;
+// cg_p_fused: rz = sum(part), p = z + (rz / sc[0]) p, sc[2] = rz;
+// cg_xr_fused: alpha = sc[2] / sum(part_pq), x += alpha p, r -= alpha q, per-CTA
+// partials of r.r into part_rr (count returned), sc[0] = sc[2].
+template <typename T> int dot_partials(long long n, const T* a, const T* b, T* part, cudaStream_t st);
+template <typename T> void cg_p_fused(long long n, const T* part, int np, T* sc, const T* z, T* p, cudaStream_t st);
+template <typename T> int cg_xr_fused(long long n, const T* part_pq, int np, T* sc, const T* p, const T* q, T* x,
+                                      T* r, T* part_rr, cudaStream_t st);
 template <typename A, typename B> void convert(long long n, const A* a, B* b, double s, cudaStream_t st);
 template <typename T> void add_to_double(long long n, const T* x, double* U, cudaStream_t st);
 template <typename KT> void impose_dirichlet(const BcDev& bc, long long ndof, double lam, const double* U, KT* K, double* R, double* dg, cudaStream_t st);
@@ -51,5 +60,11 @@ template <typename T> void dense_mv(int n, const T* M, const T* b, T* y, cudaStr
 template <typename T> void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t st);
 template <typename T> void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st);
 template <typename T> void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st);
+// Dense inverse of the coarsest operator (dense.cu): its 6 x 6 block pattern
+// (device rp, cl) and values in, the n x n row-major inverse in precision T out;
+// work holds dense_inverse_work_doubles(n) doubles.
+long long dense_inverse_work_doubles(int n);
+template <typename T> void dense_coarse_inverse(int nbrow, const int* rp, const int* cl, const T* val, int n,
+                                                double* work, T* inv, cudaStream_t st);
 
 }  // namespace pfem

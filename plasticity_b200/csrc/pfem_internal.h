@@ -76,6 +76,8 @@ struct AmgLevel {
   VT* p_val = nullptr;
   int* pslot = nullptr;   // per A block: the P block of its row whose column is agg(col)
   int *pt_rp = nullptr, *pt_blk = nullptr;  // P^T: P blocks of each aggregate
+  int* pt_row = nullptr;  // P^T order: the fine block row of each block
+  VT* pt_val = nullptr;   // P^T order: a copy of the P blocks, streamed by the restriction
   int nnzAP = 0;
   int *ap_rp = nullptr, *ap_cl = nullptr, *ap_row = nullptr;
   VT* ap_val = nullptr;
@@ -90,6 +92,7 @@ struct Amg {
   int coarse_n = 0;          // dofs of the coarsest level
   long long coarse_nnzb = 0;
   VT* coarse_val = nullptr;  // Galerkin operator of the coarsest level (6 x 6 blocks)
+  int *coarse_rp = nullptr, *coarse_cl = nullptr;  // its block pattern (device)
   VT* coarse_inv = nullptr;  // coarse_n x coarse_n dense inverse (row-major)
   VT *cx = nullptr, *cb = nullptr;
   bool built = false;
