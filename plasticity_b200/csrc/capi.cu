@@ -111,6 +111,15 @@ struct pfem_ctx {
   double* dK64 = nullptr;
   float* dK32 = nullptr;
   double* dDenseWork = nullptr;  // FP64 work matrix of the coarse dense inverse (both precisions)
+  // gathered assembly: node -> incident elements (increasing), the node's position
+  // in each, the longest block row, element-ordered tangents and forces (lazy)
+  int *dNptr = nullptr, *dNel = nullptr;
+  uint8_t* dNloc = nullptr;
+  int max_row = 0;
+  bool colored_assembly = false;
+  float* dKbuf32 = nullptr;
+  double* dKbuf64 = nullptr;
+  double* dFbuf = nullptr;
   DevStatus* dStatus = nullptr;
   // boundary conditions
   bool bcs_set = false;
@@ -1068,8 +1077,10 @@ int krylov(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, bool* 
   return PFEM_OK;
 }
 
-// One full assembly: zero K (precision prec) and R, run the element kernel over
-// every color; commit runs the state update over all elements in one launch.
+// One full assembly of K (precision prec) and R: the element kernel over every
+// element into element-ordered buffers, then the row-owned gather (or, with
+// colored_assembly, zeroed K and R and one element-kernel launch per color adding
+// in place); commit runs the state update over all elements in one launch.
 int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
   cudaStream_t st = ctx->st;
   const bool fbar = ctx->kind == PFEM_HEX8_FINITE_FBAR;
@@ -1083,6 +1094,38 @@ int assemble_dev(pfem_ctx* ctx, int prec, bool commit) {
     a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
     if (small) launch_element_small<double>(a, ctx->dAllElems, (int)ctx->ne, true, ctx->hard, st);
     else launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, true, fbar, ctx->hard, st);
+    CKL();
+    return PFEM_OK;
+  }
+  if (!ctx->colored_assembly) {
+    // one launch over every element into the element-ordered buffers, then the
+    // row-owned gather writes each block of K and each entry of R once
+    if (!ctx->dFbuf) CK(dalloc(ctx, &ctx->dFbuf, (size_t)ctx->ne * 24));
+    if (prec == PFEM_FP64) {
+      if (!ctx->dKbuf64) CK(dalloc(ctx, &ctx->dKbuf64, (size_t)ctx->ne * 576));
+      ElemArgs<double> a{};
+      a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
+      a.epsp = ctx->dEpsp; a.beta = ctx->dBeta; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+      a.R = ctx->dR; a.Kval = ctx->dK64; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
+      a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
+      a.Kbuf = ctx->dKbuf64; a.Fbuf = ctx->dFbuf;
+      if (small) launch_element_small<double>(a, ctx->dAllElems, (int)ctx->ne, false, ctx->hard, st);
+      else launch_element_color<double>(a, ctx->dAllElems, (int)ctx->ne, false, fbar, ctx->hard, st);
+      launch_gather_rows<double>((int)ctx->nn, ctx->dNptr, ctx->dNel, ctx->dNloc, ctx->dBrowptr, ctx->dRank,
+                                 ctx->dKbuf64, ctx->dFbuf, ctx->dK64, ctx->dR, ctx->max_row, st);
+    } else {
+      if (!ctx->dKbuf32) CK(dalloc(ctx, &ctx->dKbuf32, (size_t)ctx->ne * 576));
+      ElemArgs<float> a{};
+      a.X = ctx->dX; a.elem = ctx->dElem; a.U = ctx->dU; a.cpi = ctx->dCpi; a.alpha = ctx->dAlpha;
+      a.epsp = ctx->dEpsp; a.beta = ctx->dBeta; a.sigy0_e = ctx->dSigy; a.tau = ctx->dTau; a.flags = ctx->dFlags;
+      a.R = ctx->dR; a.Kval = ctx->dK32; a.browptr = ctx->dBrowptr; a.rank = ctx->dRank;
+      a.ngp = ctx->ngp; a.mat = ctx->mat; a.status = ctx->dStatus;
+      a.Kbuf = ctx->dKbuf32; a.Fbuf = ctx->dFbuf;
+      if (small) launch_element_small<float>(a, ctx->dAllElems, (int)ctx->ne, false, ctx->hard, st);
+      else launch_element_color<float>(a, ctx->dAllElems, (int)ctx->ne, false, fbar, ctx->hard, st);
+      launch_gather_rows<float>((int)ctx->nn, ctx->dNptr, ctx->dNel, ctx->dNloc, ctx->dBrowptr, ctx->dRank,
+                                ctx->dKbuf32, ctx->dFbuf, ctx->dK32, ctx->dR, ctx->max_row, st);
+    }
     CKL();
     return PFEM_OK;
   }
@@ -1678,6 +1721,23 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
   }
   UP(ctx->dColorList, clist);
   UP(ctx->dAllElems, all);
+  {
+    std::vector<uint8_t> nloc(nel.size());
+    par_for(nn, [&](long long n) {
+      for (int k = nptr[n]; k < nptr[n + 1]; ++k) {
+        const int* en = ctx->elem.data() + (long long)nel[k] * 8;
+        int a = 0;
+        while (a < 7 && en[a] != (int)n) ++a;
+        nloc[k] = (uint8_t)a;
+      }
+    });
+    UP(ctx->dNptr, nptr);
+    UP(ctx->dNel, nel);
+    UP(ctx->dNloc, nloc);
+    for (int64_t n = 0; n < nn; ++n) ctx->max_row = std::max(ctx->max_row, ctx->browptr[n + 1] - ctx->browptr[n]);
+    const char* am = getenv("PFEM_ASSEMBLY");
+    ctx->colored_assembly = am && std::string(am) == "colored";
+  }
   if (sigy0_e) {
     std::vector<double> s(sigy0_e, sigy0_e + ne);
     UP(ctx->dSigy, s);

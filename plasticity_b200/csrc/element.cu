@@ -515,10 +515,15 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
       if (a == g) { f0 = v0; f1 = v1; f2 = v2; }
     }
     if (valid) {
-      const int nd = nodes_s[warp][slot][g];
-      p.R[(long long)nd * 3 + 0] += f0;
-      p.R[(long long)nd * 3 + 1] += f1;
-      p.R[(long long)nd * 3 + 2] += f2;
+      if (p.Fbuf) {
+        double* fb = p.Fbuf + (long long)e * 24 + g * 3;
+        fb[0] = f0; fb[1] = f1; fb[2] = f2;
+      } else {
+        const int nd = nodes_s[warp][slot][g];
+        p.R[(long long)nd * 3 + 0] += f0;
+        p.R[(long long)nd * 3 + 1] += f1;
+        p.R[(long long)nd * 3 + 2] += f2;
+      }
     }
     // ---- A = dP/dFbar in the eigenbasis of b^e (dPdF, FiniteStrain.jl:503-547) ----
     // gamma_AB of _dhalflog_contract (FiniteStrain.jl:463-482)
@@ -706,6 +711,16 @@ element_color_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) acc[a * 3 + i] += x0 * T[i] + x1 * T[3 + i] + x2 * T[6 + i];
       }
+    }
+    if (p.Kbuf) {
+      // element-ordered: column (b,k) of rows (a,i) at [es][a][i][col]; the 24
+      // lanes of an element write 24 consecutive values per (a,i)
+      KT* kb = p.Kbuf + (long long)es * 576 + col;
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) __stcs(kb + a * 72 + i * 24, (KT)acc[a * 3 + i]);
+      continue;
     }
     // The eight target blocks lie in eight different block rows, so nothing
     // aliases: all 24 loads are issued before any store (one memory latency
@@ -914,10 +929,15 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
       if (a == g) { f0 = v0; f1 = v1; f2 = v2; }
     }
     if (valid) {
-      const int nd = nodes_s[warp][slot][g];
-      p.R[(long long)nd * 3 + 0] += f0;
-      p.R[(long long)nd * 3 + 1] += f1;
-      p.R[(long long)nd * 3 + 2] += f2;
+      if (p.Fbuf) {
+        double* fb = p.Fbuf + (long long)e * 24 + g * 3;
+        fb[0] = f0; fb[1] = f1; fb[2] = f2;
+      } else {
+        const int nd = nodes_s[warp][slot][g];
+        p.R[(long long)nd * 3 + 0] += f0;
+        p.R[(long long)nd * 3 + 1] += f1;
+        p.R[(long long)nd * 3 + 2] += f2;
+      }
     }
     // ---- w D: D = C - 3G b0 Idev + 3G (b0 - g0) n n^T (Materials.jl:245-247) ----
 #pragma unroll
@@ -971,6 +991,14 @@ element_small_kernel(ElemArgs<KT> p, const int* __restrict__ elist, int nlist) {
           acc[a * 3 + 1] += x1 * T[1] + x0 * T[3] + x2 * T[4];
           acc[a * 3 + 2] += x2 * T[2] + x1 * T[4] + x0 * T[5];
         }
+      }
+      if (p.Kbuf) {
+        KT* kb = p.Kbuf + (long long)es * 576 + col;
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) __stcs(kb + a * 72 + i * 24, (KT)acc[a * 3 + i]);
+        continue;
       }
       const int* nds = nodes_s[warp][s2];
       KT* vp[8];
@@ -1042,6 +1070,66 @@ void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool c
   else if (hard == HARD_VOCE) launch_color_h<KT, HARD_VOCE>(a, elist, n, commit, fbar, st);
   else launch_color_h<KT, HARD_LINEAR>(a, elist, n, commit, fbar, st);
 }
+
+// ---------------------------------------------------------------- row gather
+// One warp per node a: the row's blocks accumulate in shared memory, element by
+// element in increasing element order (a fixed order: deterministic sums).
+// Within one element the 72 values go to 72 distinct entries (eight distinct
+// column nodes), so the lanes never add into the same entry at once.
+template <typename KT>
+__global__ void __launch_bounds__(256) gather_rows_kernel(int nn, const int* __restrict__ nptr,
+                                                          const int* __restrict__ nel,
+                                                          const uint8_t* __restrict__ nloc,
+                                                          const int* __restrict__ browptr,
+                                                          const uint8_t* __restrict__ rank,
+                                                          const KT* __restrict__ Kbuf,
+                                                          const double* __restrict__ Fbuf, KT* __restrict__ Kval,
+                                                          double* __restrict__ R, int maxlen) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = (int)blockIdx.x * (int)(blockDim.x >> 5) + warp;
+  if (a >= nn) return;  // whole warps; no block-wide barrier below
+  KT* acc = reinterpret_cast<KT*>(gsm) + (size_t)warp * maxlen * 9;
+  const int r0 = browptr[a], len9 = (browptr[a + 1] - r0) * 9;
+  for (int v = lane; v < len9; v += 32) acc[v] = KT(0);
+  double fr = 0.0;
+  __syncwarp();
+  const int q1 = nptr[a + 1];
+  for (int q = nptr[a]; q < q1; ++q) {
+    const int e = nel[q];
+    const int al = nloc[q];
+    const KT* src = Kbuf + (long long)e * 576 + al * 72;
+    const uint8_t* rk = rank + (long long)e * 64 + al * 8;
+    for (int v = lane; v < 72; v += 32) {
+      const int i = v / 24, col = v - 24 * i, b = col / 3, k = col - 3 * b;
+      acc[rk[b] * 9 + i * 3 + k] += __ldcs(src + v);
+    }
+    if (lane < 3) fr += Fbuf[(long long)e * 24 + al * 3 + lane];
+    __syncwarp();
+  }
+  KT* dst = Kval + (long long)r0 * 9;
+  for (int v = lane; v < len9; v += 32) dst[v] = acc[v];
+  if (lane < 3) R[(long long)a * 3 + lane] = fr;
+}
+
+template <typename KT>
+void launch_gather_rows(int nn, const int* nptr, const int* nel, const uint8_t* nloc, const int* browptr,
+                        const uint8_t* rank, const KT* Kbuf, const double* Fbuf, KT* Kval, double* R, int maxlen,
+                        cudaStream_t st) {
+  constexpr int WARPS = 8;
+  const size_t sm = (size_t)WARPS * maxlen * 9 * sizeof(KT);
+  const int blocks = (nn + WARPS - 1) / WARPS;
+  if (blocks <= 0) return;
+  if (sm > 48 * 1024)  // rows longer than a hex mesh's 27 blocks (the 8-bit rank table caps them at 256)
+    cudaFuncSetAttribute(gather_rows_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  pfem::count_launch();
+  gather_rows_kernel<KT><<<blocks, 32 * WARPS, sm, st>>>(nn, nptr, nel, nloc, browptr, rank, Kbuf, Fbuf, Kval, R,
+                                                        maxlen);
+}
+template void launch_gather_rows<double>(int, const int*, const int*, const uint8_t*, const int*, const uint8_t*,
+                                         const double*, const double*, double*, double*, int, cudaStream_t);
+template void launch_gather_rows<float>(int, const int*, const int*, const uint8_t*, const int*, const uint8_t*,
+                                        const float*, const double*, float*, double*, int, cudaStream_t);
 
 template void launch_element_color<double>(const ElemArgs<double>&, const int*, int, bool, bool, int, cudaStream_t);
 template void launch_element_color<float>(const ElemArgs<float>&, const int*, int, bool, bool, int, cudaStream_t);

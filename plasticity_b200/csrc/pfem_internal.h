@@ -26,6 +26,11 @@ struct ElemArgs {
   KT* Kval;                // nnzb x 9 block-CSR tangent values (accumulated)
   const int* browptr;      // nn+1 block row pointers
   const uint8_t* rank;     // ne x 64: position of node b in node a's block row
+  // Element-ordered outputs (the gathered assembly): when set, the kernel writes
+  // K_e as Kbuf[e][a][i][(b,k)] (576 values: rows of node a together) and F_e as
+  // Fbuf[e][a][i] (24 doubles) instead of adding into Kval and R.
+  KT* Kbuf;
+  double* Fbuf;
   long long ngp;
   MatParams mat;
   DevStatus* status;
@@ -39,6 +44,15 @@ void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool c
 template <typename KT>
 void launch_element_small(const ElemArgs<KT>& a, const int* elist, int n, bool commit, int hard,
                           cudaStream_t st);
+
+// Row-owned gather (element.cu): block row a of K and R[a] are the sums, over
+// the elements incident to node a in increasing element order (nptr/nel, with
+// nloc the node's position in the element), of the element buffers' (a, b)
+// blocks and force rows.  Every block of K and every entry of R is written once.
+template <typename KT>
+void launch_gather_rows(int nn, const int* nptr, const int* nel, const uint8_t* nloc, const int* browptr,
+                        const uint8_t* rank, const KT* Kbuf, const double* Fbuf, KT* Kval, double* R, int maxlen,
+                        cudaStream_t st);
 
 // One-time topology on the device (topology.cu): per-node block rows
 // (count pass with col = null, fill pass with rowptr) and the rank table.
