@@ -1,7 +1,10 @@
 // mlp.cu -- learned per-node Newton predictor: 12 -> 128 -> 128 -> 3 MLP (GELU)
 // on BF16 tensor cores (tcgen05.mma kind::f16, FP32 accumulation in TMEM).
 //
-// One CTA (4 warps, one thread per tile row) loops over tiles of 128 samples.
+// One CTA (8 warps: two threads per tile row, each taking half of the row's
+// columns in the epilogues) loops over tiles of 128 samples.  The forward-only
+// kernel keeps H2 in H1's tile and allocates 256 TMEM columns, so two CTAs share
+// an SM and one's epilogue overlaps the other's MMAs.
 // Forward:  Z1 = X W1^T + b1, H1 = gelu(Z1); Z2 = H1 W2^T + b2, H2 = gelu(Z2);
 //           Y = H2 W3^T + b3.
 // Backward (mean squared error over the 3 outputs):
@@ -41,23 +44,30 @@ constexpr int OFF_W3 = OFF_B2 + HID;            // [OUTP][HID]
 constexpr int OFF_B3 = OFF_W3 + OUTP * HID;     // [OUTP]
 static_assert(OFF_B3 + OUTP == MLP_NPARAMS, "parameter layout");
 
-// shared-memory map (bytes)
-constexpr int S_W1 = 0;                         // 128 x 16
-constexpr int S_W2 = S_W1 + HID * INP * 2;      // 128 x 128
-constexpr int S_W3 = S_W2 + HID * HID * 2;      // 16 x 128
-constexpr int S_X = S_W3 + OUTP * HID * 2;      // 128 x 16
-constexpr int S_H1 = S_X + TR * INP * 2;        // 128 x 128
-constexpr int S_H2 = S_H1 + TR * HID * 2;
-constexpr int S_DY = S_H2 + TR * HID * 2;       // 128 x 16
-constexpr int S_DZ2 = S_DY + TR * OUTP * 2;     // 128 x 128
-constexpr int S_DZ1 = S_DZ2 + TR * HID * 2;
-constexpr int S_BIAS = S_DZ1 + TR * HID * 2;    // b1, b2, b3 floats
-constexpr int S_DB = S_BIAS + (HID + HID + OUTP) * 4;  // db1, db2, db3 partials
-constexpr int S_MISC = S_DB + (HID + HID + OUTP) * 4;  // mbarrier, tmem base, abort, loss
-constexpr int SMEM_TOTAL = S_MISC + 64;
+constexpr int NT = 256;   // threads per CTA: row = tid % 128, column half = tid / 128
+
+// shared-memory map (bytes); the forward-only kernel writes H2 over H1 (the
+// MMA that reads H1 has completed by then) and has no backward tiles
+template <bool TRAIN>
+struct Lay {
+  static constexpr int W1 = 0;                               // 128 x 16
+  static constexpr int W2 = W1 + HID * INP * 2;              // 128 x 128
+  static constexpr int W3 = W2 + HID * HID * 2;              // 16 x 128
+  static constexpr int X = W3 + OUTP * HID * 2;              // 128 x 16
+  static constexpr int H1 = X + TR * INP * 2;                // 128 x 128
+  static constexpr int H2 = TRAIN ? H1 + TR * HID * 2 : H1;
+  static constexpr int DY = H2 + TR * HID * 2;               // 128 x 16
+  static constexpr int DZ2 = DY + (TRAIN ? TR * OUTP * 2 : 0);
+  static constexpr int DZ1 = DZ2 + (TRAIN ? TR * HID * 2 : 0);
+  static constexpr int BIAS = DZ1 + (TRAIN ? TR * HID * 2 : 0);  // b1, b2, b3 floats
+  static constexpr int DB = BIAS + (HID + HID + OUTP) * 4;       // db1, db2, db3 partials
+  static constexpr int MISC = DB + (HID + HID + OUTP) * 4;       // mbarrier, tmem base, abort, loss
+  static constexpr int TOTAL = MISC + 64;
+  static constexpr uint32_t COLS = TRAIN ? 512 : 256;            // TMEM columns allocated
+};
 
 // TMEM columns
-constexpr uint32_t T_DA = 0, T_DB = 128, T_G2 = 256, T_G1 = 384, T_G3 = 400, T_COLS = 512;
+constexpr uint32_t T_DA = 0, T_DB = 128, T_G2 = 256, T_G1 = 384, T_G3 = 400;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -147,6 +157,32 @@ __device__ __forceinline__ void store16(unsigned char* tile, int r, int c0, int 
   }
 }
 
+// Column sums over the warp's 32 rows of 16 per-lane values, by halving
+// exchanges (8 + 4 + 2 + 1 + 1 shuffles): afterwards the even lane 2m holds the
+// sum of column colsum16_col(2m); returns it (odd lanes hold the same value).
+__device__ __forceinline__ int colsum16_col(int lane) {
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+__device__ __forceinline__ float colsum16(const float* v16, int lane) {
+  float v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = v16[i];
+#pragma unroll
+  for (int o = 16, m = 16; o >= 2; o >>= 1, m >>= 1) {
+    const bool lower = (lane & o) == 0;
+    const int half = m >> 1;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      if (i < half) {
+        const float send = lower ? v[i + half] : v[i];
+        const float recv = __shfl_xor_sync(0xffffffffu, send, o);
+        v[i] = (lower ? v[i] : v[i + half]) + recv;
+      }
+    }
+  }
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
 struct Ctl {
   uint32_t mbar;
   uint32_t phase;
@@ -170,33 +206,37 @@ __device__ __forceinline__ void sync_threads_tc() {
 }
 
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(NT, 1)
 mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restrict__ X, const float* __restrict__ T,
                 const int* __restrict__ rows, long long nrows, float* __restrict__ Y, float* __restrict__ grad,
                 float* __restrict__ loss, float inv_scale, int* __restrict__ err) {
+  using LY = Lay<TRAIN>;
   extern __shared__ __align__(1024) unsigned char sm[];
   const int tid = threadIdx.x;
-  float* bias = reinterpret_cast<float*>(sm + S_BIAS);
-  float* dbias = reinterpret_cast<float*>(sm + S_DB);
-  uint64_t* mbar_p = reinterpret_cast<uint64_t*>(sm + S_MISC);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + S_MISC + 8);
-  int* abort_flag = reinterpret_cast<int*>(sm + S_MISC + 12);
-  float* loss_s = reinterpret_cast<float*>(sm + S_MISC + 16);
+  const int row = tid & (TR - 1);         // tile row = TMEM lane
+  const int half = tid >> 7;              // which 64 of the 128 hidden columns this thread handles
+  const int lane = tid & 31;
+  float* bias = reinterpret_cast<float*>(sm + LY::BIAS);
+  float* dbias = reinterpret_cast<float*>(sm + LY::DB);
+  uint64_t* mbar_p = reinterpret_cast<uint64_t*>(sm + LY::MISC);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + LY::MISC + 8);
+  int* abort_flag = reinterpret_cast<int*>(sm + LY::MISC + 12);
+  float* loss_s = reinterpret_cast<float*>(sm + LY::MISC + 16);
 
   // ---- weights (BF16, K-major tiles) and biases into shared memory ----
-  for (int i = tid; i < HID * INP; i += 128) {
+  for (int i = tid; i < HID * INP; i += NT) {
     const int r = i / INP, c = i % INP;
-    *reinterpret_cast<__nv_bfloat16*>(sm + S_W1 + tile_off(r, c, HID)) = __float2bfloat16_rn(params[OFF_W1 + i]);
+    *reinterpret_cast<__nv_bfloat16*>(sm + LY::W1 + tile_off(r, c, HID)) = __float2bfloat16_rn(params[OFF_W1 + i]);
   }
-  for (int i = tid; i < HID * HID; i += 128) {
+  for (int i = tid; i < HID * HID; i += NT) {
     const int r = i / HID, c = i % HID;
-    *reinterpret_cast<__nv_bfloat16*>(sm + S_W2 + tile_off(r, c, HID)) = __float2bfloat16_rn(params[OFF_W2 + i]);
+    *reinterpret_cast<__nv_bfloat16*>(sm + LY::W2 + tile_off(r, c, HID)) = __float2bfloat16_rn(params[OFF_W2 + i]);
   }
-  for (int i = tid; i < OUTP * HID; i += 128) {
+  for (int i = tid; i < OUTP * HID; i += NT) {
     const int r = i / HID, c = i % HID;
-    *reinterpret_cast<__nv_bfloat16*>(sm + S_W3 + tile_off(r, c, OUTP)) = __float2bfloat16_rn(params[OFF_W3 + i]);
+    *reinterpret_cast<__nv_bfloat16*>(sm + LY::W3 + tile_off(r, c, OUTP)) = __float2bfloat16_rn(params[OFF_W3 + i]);
   }
-  for (int i = tid; i < HID + HID + OUTP; i += 128) {
+  for (int i = tid; i < HID + HID + OUTP; i += NT) {
     bias[i] = i < HID ? params[OFF_B1 + i] : (i < 2 * HID ? params[OFF_B2 + i - HID] : params[OFF_B3 + i - 2 * HID]);
     dbias[i] = 0.0f;
   }
@@ -208,16 +248,17 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
   }
   if (tid < 32) {  // warp 0 allocates TMEM
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
-                 "r"(T_COLS));
+                 "r"(LY::COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   sync_threads_tc();
   const uint32_t tbase = *tmem_slot;
-  const uint32_t lane_off = (uint32_t)((tid & ~31) << 16);  // this warp's TMEM lanes
+  const uint32_t lane_off = (uint32_t)((row & ~31) << 16);  // this warp's TMEM lanes
   Ctl ctl{smem_addr(mbar_p), 0u, true};
-  const uint32_t aW1 = smem_addr(sm + S_W1), aW2 = smem_addr(sm + S_W2), aW3 = smem_addr(sm + S_W3);
-  const uint32_t aX = smem_addr(sm + S_X), aH1 = smem_addr(sm + S_H1), aH2 = smem_addr(sm + S_H2);
-  const uint32_t aDY = smem_addr(sm + S_DY), aDZ2 = smem_addr(sm + S_DZ2), aDZ1 = smem_addr(sm + S_DZ1);
+  const uint32_t aW1 = smem_addr(sm + LY::W1), aW2 = smem_addr(sm + LY::W2), aW3 = smem_addr(sm + LY::W3);
+  const uint32_t aX = smem_addr(sm + LY::X), aH1 = smem_addr(sm + LY::H1), aH2 = smem_addr(sm + LY::H2);
+  const uint32_t aDY = smem_addr(sm + LY::DY), aDZ2 = smem_addr(sm + LY::DZ2), aDZ1 = smem_addr(sm + LY::DZ1);
+  const int c_lo = half * (HID / 2), c_hi = c_lo + HID / 2;  // this thread's hidden columns
   bool first_tile = true;
   const long long ntiles = (nrows + TR - 1) / TR;
   float lsum = 0.0f;
@@ -227,42 +268,42 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
     __syncthreads();
     if (*abort_flag) break;
     const long long row0 = tile * TR;
-    const long long gr = row0 + tid;
+    const long long gr = row0 + row;
     const bool valid = gr < nrows;
     const long long src = valid ? (rows ? (long long)rows[gr] : gr) : 0;
     // ---- X tile ----
-    {
+    if (half == 0) {
       uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
       if (valid) {
         const uint4* p = reinterpret_cast<const uint4*>(X + src * INP);
         a = p[0];
         b = p[1];
       }
-      *reinterpret_cast<uint4*>(sm + S_X + tile_off(tid, 0, TR)) = a;
-      *reinterpret_cast<uint4*>(sm + S_X + tile_off(tid, 8, TR)) = b;
+      *reinterpret_cast<uint4*>(sm + LY::X + tile_off(row, 0, TR)) = a;
+      *reinterpret_cast<uint4*>(sm + LY::X + tile_off(row, 8, TR)) = b;
     }
     sync_threads_tc();
     // ---- Z1 = X W1^T ----
     if (tid == 0) mma(tbase + T_DA, desc_k(aX, TR, 0), desc_k(aW1, HID, 0), idesc(HID, 0, 0), 0);
     sync_mma(ctl, err, abort_flag);
-    for (int c = 0; c < HID; c += 16) {
+    for (int c = c_lo; c < c_hi; c += 16) {
       float v[16];
       tmem_ld16(tbase + lane_off + T_DA + c, v);
 #pragma unroll
       for (int i = 0; i < 16; ++i) v[i] = gelu(v[i] + bias[c + i]);
-      store16(sm + S_H1, tid, c, TR, v);
+      store16(sm + LY::H1, row, c, TR, v);
     }
     sync_threads_tc();
     // ---- Z2 = H1 W2^T ----
     if (tid == 0)
       for (int s = 0; s < HID / 16; ++s) mma(tbase + T_DB, desc_k(aH1, TR, s), desc_k(aW2, HID, s), idesc(HID, 0, 0), s > 0);
     sync_mma(ctl, err, abort_flag);
-    for (int c = 0; c < HID; c += 16) {
+    for (int c = c_lo; c < c_hi; c += 16) {
       float v[16];
       tmem_ld16(tbase + lane_off + T_DB + c, v);
 #pragma unroll
       for (int i = 0; i < 16; ++i) v[i] = gelu(v[i] + bias[HID + c + i]);
-      store16(sm + S_H2, tid, c, TR, v);
+      store16(sm + LY::H2, row, c, TR, v);
     }
     sync_threads_tc();
     // ---- Y = H2 W3^T ----
@@ -274,7 +315,7 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
 #pragma unroll
     for (int i = 0; i < 16; ++i) y[i] += bias[2 * HID + i];
     if constexpr (!TRAIN) {
-      if (valid) {
+      if (valid && half == 0) {
         Y[gr * 3 + 0] = y[0];
         Y[gr * 3 + 1] = y[1];
         Y[gr * 3 + 2] = y[2];
@@ -285,7 +326,7 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
     float dy[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) dy[i] = 0.0f;
-    if (valid) {
+    if (valid && half == 0) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         const float e = y[j] - T[src * 3 + j];
@@ -293,9 +334,11 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
         dy[j] = 2.0f * e * inv_scale;
       }
     }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) atomicAdd(&dbias[2 * HID + j], dy[j]);
-    store16(sm + S_DY, tid, 0, TR, dy);
+    {
+      const float cs = colsum16(dy, lane);  // warps of the upper half contribute zeros
+      if (half == 0 && (lane & 1) == 0 && colsum16_col(lane) < 3) atomicAdd(&dbias[2 * HID + colsum16_col(lane)], cs);
+    }
+    if (half == 0) store16(sm + LY::DY, row, 0, TR, dy);
     sync_threads_tc();
     // dH2 = dY W3 (W3 as MN-major B), dW3^T += H2^T dY
     if (tid == 0) {
@@ -304,16 +347,15 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
         mma(tbase + T_G3, desc_mn(aH2, TR, s), desc_mn(aDY, TR, s), idesc(OUTP, 1, 1), (s > 0) || !first_tile);
     }
     sync_mma(ctl, err, abort_flag);
-    for (int c = 0; c < HID; c += 16) {
+    for (int c = c_lo; c < c_hi; c += 16) {
       float g[16], z[16];
       tmem_ld16(tbase + lane_off + T_DA + c, g);
       tmem_ld16(tbase + lane_off + T_DB + c, z);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        g[i] = valid ? g[i] * gelu_d(z[i] + bias[HID + c + i]) : 0.0f;
-        atomicAdd(&dbias[HID + c + i], g[i]);
-      }
-      store16(sm + S_DZ2, tid, c, TR, g);
+      for (int i = 0; i < 16; ++i) g[i] = valid ? g[i] * gelu_d(z[i] + bias[HID + c + i]) : 0.0f;
+      const float cs = colsum16(g, lane);
+      if ((lane & 1) == 0) atomicAdd(&dbias[HID + c + colsum16_col(lane)], cs);
+      store16(sm + LY::DZ2, row, c, TR, g);
     }
     sync_threads_tc();
     // dH1 = dZ2 W2, dW2 += dZ2^T H1, Z1 again = X W1^T
@@ -324,16 +366,15 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
       mma(tbase + T_DA, desc_k(aX, TR, 0), desc_k(aW1, HID, 0), idesc(HID, 0, 0), 0);
     }
     sync_mma(ctl, err, abort_flag);
-    for (int c = 0; c < HID; c += 16) {
+    for (int c = c_lo; c < c_hi; c += 16) {
       float g[16], z[16];
       tmem_ld16(tbase + lane_off + T_DB + c, g);
       tmem_ld16(tbase + lane_off + T_DA + c, z);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        g[i] = valid ? g[i] * gelu_d(z[i] + bias[c + i]) : 0.0f;
-        atomicAdd(&dbias[c + i], g[i]);
-      }
-      store16(sm + S_DZ1, tid, c, TR, g);
+      for (int i = 0; i < 16; ++i) g[i] = valid ? g[i] * gelu_d(z[i] + bias[c + i]) : 0.0f;
+      const float cs = colsum16(g, lane);
+      if ((lane & 1) == 0) atomicAdd(&dbias[c + colsum16_col(lane)], cs);
+      store16(sm + LY::DZ1, row, c, TR, g);
     }
     sync_threads_tc();
     // dW1 += dZ1^T X
@@ -347,23 +388,25 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
 
   if (TRAIN && !first_tile && !*abort_flag) {
     // weight gradients: TMEM lane = hidden unit (row of W1 / W2, column of W3)
-    for (int c = 0; c < HID; c += 16) {
+    for (int c = c_lo; c < c_hi; c += 16) {
       float g[16];
       tmem_ld16(tbase + lane_off + T_G2 + c, g);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) atomicAdd(&grad[OFF_W2 + tid * HID + c + i], g[i]);
+      for (int i = 0; i < 16; ++i) atomicAdd(&grad[OFF_W2 + row * HID + c + i], g[i]);
     }
     {
       float g[16];
-      tmem_ld16(tbase + lane_off + T_G1, g);
+      tmem_ld16(tbase + lane_off + (half == 0 ? T_G1 : T_G3), g);
+      if (half == 0) {
 #pragma unroll
-      for (int i = 0; i < 16; ++i) atomicAdd(&grad[OFF_W1 + tid * INP + i], g[i]);
-      tmem_ld16(tbase + lane_off + T_G3, g);
+        for (int i = 0; i < 16; ++i) atomicAdd(&grad[OFF_W1 + row * INP + i], g[i]);
+      } else {
 #pragma unroll
-      for (int i = 0; i < 16; ++i) atomicAdd(&grad[OFF_W3 + i * HID + tid], g[i]);
+        for (int i = 0; i < 16; ++i) atomicAdd(&grad[OFF_W3 + i * HID + row], g[i]);
+      }
     }
     __syncthreads();
-    for (int i = tid; i < HID + HID + OUTP; i += 128) {
+    for (int i = tid; i < HID + HID + OUTP; i += NT) {
       const int off = i < HID ? OFF_B1 + i : (i < 2 * HID ? OFF_B2 + i - HID : OFF_B3 + i - 2 * HID);
       atomicAdd(&grad[off], dbias[i]);
     }
@@ -373,7 +416,7 @@ mlp_tile_kernel(const float* __restrict__ params, const __nv_bfloat16* __restric
   }
   fence_before();
   __syncthreads();
-  if (tid < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(T_COLS));
+  if (tid < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(LY::COLS));
 }
 
 // Adam (FP32 master weights); bias-corrected step.
@@ -550,22 +593,26 @@ void mlp_random_rows(int n, long long nrows, unsigned long long seed, int* rows,
   random_rows_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, nrows, seed, rows);
 }
 
-size_t mlp_smem_bytes() { return (size_t)SMEM_TOTAL; }
+size_t mlp_smem_bytes() { return (size_t)Lay<true>::TOTAL; }
 
 int mlp_launch(bool train, const float* params, const void* X, const float* T, const int* rows, long long nrows,
                float* Y, float* grad, float* loss, int* err, int max_ctas, cudaStream_t st) {
   if (nrows <= 0) return 0;
   const long long ntiles = (nrows + TR - 1) / TR;
-  const int grid = (int)std::min<long long>(ntiles, max_ctas);
+  // max_ctas is a count of SMs: the training kernel (512 TMEM columns, ~178 KB of
+  // shared memory) runs one CTA per SM, the forward kernel (256 columns, ~80 KB) two
+  const int grid = (int)std::min<long long>(ntiles, (long long)max_ctas * (train ? 1 : 2));
   const float inv_scale = 1.0f / (3.0f * (float)nrows);
   const __nv_bfloat16* Xb = static_cast<const __nv_bfloat16*>(X);
   count_launch();
   if (train) {
-    cudaFuncSetAttribute(mlp_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TOTAL);
-    mlp_tile_kernel<true><<<grid, 128, SMEM_TOTAL, st>>>(params, Xb, T, rows, nrows, Y, grad, loss, inv_scale, err);
+    cudaFuncSetAttribute(mlp_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay<true>::TOTAL);
+    mlp_tile_kernel<true><<<grid, NT, Lay<true>::TOTAL, st>>>(params, Xb, T, rows, nrows, Y, grad, loss, inv_scale,
+                                                              err);
   } else {
-    cudaFuncSetAttribute(mlp_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TOTAL);
-    mlp_tile_kernel<false><<<grid, 128, SMEM_TOTAL, st>>>(params, Xb, T, rows, nrows, Y, grad, loss, inv_scale, err);
+    cudaFuncSetAttribute(mlp_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay<false>::TOTAL);
+    mlp_tile_kernel<false><<<grid, NT, Lay<false>::TOTAL, st>>>(params, Xb, T, rows, nrows, Y, grad, loss, inv_scale,
+                                                                err);
   }
   return (int)cudaGetLastError();
 }
