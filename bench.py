@@ -191,27 +191,21 @@ def run_increments(M, w, first, last, maxiter=40, **kw):
 def cpu_reference(n_cpu, increments, tol, nthreads=0):
     """Whole load increments of the reference's algorithm on the CPU oracle: the
     C++ restatement of assembly + Dirichlet imposition on all host threads, the
-    linear solve by SuperLU (sequential; stands in for UMFPACK,
-    Solver.jl:237-240), the previous converged U as predictor (Solver.jl:321-323)
-    and the commit re-assembly (Solver.jl:470-471), on the same workload generator
-    at n_cpu^3.  Returns per-increment (newton iterations, seconds) and phase times."""
+    linear solve by SuperLU in a nested-dissection order (sequential; stands in
+    for UMFPACK, Solver.jl:237-240), the previous converged U as predictor
+    (Solver.jl:321-323) and the commit re-assembly (Solver.jl:470-471), on the same
+    workload generator at n_cpu^3.  Returns the workload, per-increment (Newton
+    iterations, seconds) and the LU seconds."""
     from oracle import oracle as O
     from plasticity_b200 import workloads as W
-    import scipy.sparse.linalg as spla
     O.build()
     w = W.config2(n=n_cpu)
     om = O.OracleModel(w.mesh.nodes, w.mesh.elements, O.J2Material(**w.material), fbar=True,
                        sigy0_e=w.sigy0_e, nthreads=nthreads)
     w.apply(om)
     ramp, fix = om.freeze_bcs()
-    t_lu = [0.0]
-
-    def lu(K, b):
-        t0 = time.perf_counter()
-        x = spla.splu(K.tocsc(), permc_spec="MMD_AT_PLUS_A").solve(b)
-        t_lu[0] += time.perf_counter() - t0
-        return x
-
+    stats = {}
+    lu = O.nd_lu_solver(O.box_nd_dofs(n_cpu, n_cpu, n_cpu), stats)
     out = []
     for s in increments:
         t0 = time.perf_counter()
@@ -221,7 +215,7 @@ def cpu_reference(n_cpu, increments, tol, nthreads=0):
         _, _, tau, fl = om.assemble(om.U, commit=True)
         om.tau, om.flags = tau, fl
         out.append((len(hist), time.perf_counter() - t0))
-    return w, out, t_lu[0]
+    return w, out, stats.get("lu_s", 0.0)
 
 
 def lscpu_summary():
@@ -245,10 +239,10 @@ def cpu_baseline(n_cpu, first, last, tol):
             "sample": (f"increments {first}..{last} of {w.nsteps} of the same workload generator at {n_cpu}^3 "
                        f"({3 * w.mesh.nnodes} DOF), whole increments end to end: the reference algorithm "
                        f"(previous-U predictor, exact LU every Newton iteration, no line search) on the C++ "
-                       f"oracle (assembly + imposition on {os.cpu_count()} threads) with SuperLU (sequential) "
-                       f"standing in for UMFPACK; Newton iterations {newton}, LU {t_lu:.1f} s of {secs:.1f} s. "
-                       f"The bench mesh (64^3, 823,875 DOF) is out of reach of a direct LU in the budget "
-                       f"(SuperLU time grows ~N^2: 0.35 / 1.7 / 7.2 s per factorisation at 12^3 / 16^3 / 20^3)"),
+                       f"oracle (assembly + imposition on {os.cpu_count()} threads) with SuperLU (sequential, "
+                       f"nested-dissection order) standing in for UMFPACK; Newton iterations {newton}, LU "
+                       f"{t_lu:.1f} s of {secs:.1f} s. The bench mesh (64^3, 823,875 DOF) is out of reach of a "
+                       f"direct LU in the budget (factorisation time grows ~N^2: 1.0 / 3.4 s at 16^3 / 20^3)"),
             "mesh": f"{n_cpu}^3", "newton_iters": newton, "seconds": secs, "lu_seconds": t_lu,
             "lscpu": lscpu_summary()}
 
@@ -260,7 +254,6 @@ def reference_arm(args, config):
     nsteps = W.config2(n=n_cpu).nsteps
     first = args.warmup + 1
     last = min(args.warmup + args.steps, nsteps)
-    _, warm, _ = cpu_reference(n_cpu, range(1, 1), 1e-10)  # builds the oracle
     t_all = time.perf_counter()
     w, out, t_lu = cpu_reference(n_cpu, range(1, last + 1), 1e-10)
     timed = out[first - 1:]
@@ -275,8 +268,8 @@ def reference_arm(args, config):
             "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": "load-steps/s", "cores": os.cpu_count(), "kind": "port",
                              "sample": f"increments {first}..{last} of {nsteps} at {n_cpu}^3, whole increments: "
-                                       f"C++ oracle assembly on all threads + SuperLU (sequential) in place of "
-                                       f"UMFPACK, previous-U predictor; Newton iterations "
+                                       f"C++ oracle assembly on all threads + SuperLU (sequential, nested-dissection "
+                                       f"order) in place of UMFPACK, previous-U predictor; Newton iterations "
                                        f"{[k for k, _ in timed]}; total run {time.perf_counter() - t_all:.1f} s",
                              "lscpu": lscpu_summary()},
             "e2e": {"value": value, "unit": "load-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
