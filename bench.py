@@ -188,7 +188,21 @@ def run_increments(M, w, first, last, maxiter=40, **kw):
     return its
 
 
-def cpu_reference(n_cpu, increments, tol, nthreads=0):
+WORKLOADS = ("compress", "indent")
+
+
+def make_workload(kind, n):
+    """The bench workloads: 'compress' is the 64^3 jittered / lognormal cube under
+    20 % top-face compression in 40 increments; 'indent' is the 150^3 cube of the
+    same kind with a central 30 x 30-node top-face patch indented 10 % in 30
+    increments (the patch scales with the mesh below 150^3)."""
+    from plasticity_b200 import workloads as W
+    if kind == "compress":
+        return W.config2(n=n)
+    return W.config3(n=n, patch=max(2, round(30 * n / 150)))
+
+
+def cpu_reference(n_cpu, increments, tol, nthreads=0, kind="compress"):
     """Whole load increments of the reference's algorithm on the CPU oracle: the
     C++ restatement of assembly + Dirichlet imposition on all host threads, the
     linear solve by SuperLU in a nested-dissection order (sequential; stands in
@@ -197,9 +211,8 @@ def cpu_reference(n_cpu, increments, tol, nthreads=0):
     workload generator at n_cpu^3.  Returns the workload, per-increment (Newton
     iterations, seconds) and the LU seconds."""
     from oracle import oracle as O
-    from plasticity_b200 import workloads as W
     O.build()
-    w = W.config2(n=n_cpu)
+    w = make_workload(kind, n_cpu)
     om = O.OracleModel(w.mesh.nodes, w.mesh.elements, O.J2Material(**w.material), fbar=True,
                        sigy0_e=w.sigy0_e, nthreads=nthreads)
     w.apply(om)
@@ -209,7 +222,10 @@ def cpu_reference(n_cpu, increments, tol, nthreads=0):
     out = []
     for s in increments:
         t0 = time.perf_counter()
-        conv, hist = om.newton(s / w.nsteps, ramp, fix, tol, 40, linsolve=lu)
+        # the indentation's patch edge inverts elements under plain Newton from the
+        # previous U; there the baseline takes the same backtracking line search as
+        # the GPU arms (the reference has none and stops)
+        conv, hist = om.newton(s / w.nsteps, ramp, fix, tol, 40, linsolve=lu, line_search=kind == "indent")
         if not conv:
             raise RuntimeError(f"CPU reference: increment {s} at {n_cpu}^3 did not converge")
         _, _, tau, fl = om.assemble(om.U, commit=True)
@@ -231,17 +247,18 @@ def lscpu_summary():
         return {}
 
 
-def cpu_baseline(n_cpu, first, last, tol):
-    w, out, t_lu = cpu_reference(n_cpu, range(first, last + 1), tol)
+def cpu_baseline(n_cpu, first, last, tol, kind="compress", bench_mesh="64^3, 823,875 DOF"):
+    w, out, t_lu = cpu_reference(n_cpu, range(first, last + 1), tol, kind=kind)
     secs = sum(t for _, t in out)
     newton = [k for k, _ in out]
     return {"value": len(out) / secs, "unit": "load-steps/s", "cores": os.cpu_count(), "kind": "port",
             "sample": (f"increments {first}..{last} of {w.nsteps} of the same workload generator at {n_cpu}^3 "
                        f"({3 * w.mesh.nnodes} DOF), whole increments end to end: the reference algorithm "
-                       f"(previous-U predictor, exact LU every Newton iteration, no line search) on the C++ "
+                       f"(previous-U predictor, exact LU every Newton iteration, "
+                       f"{'backtracking line search' if kind == 'indent' else 'no line search'}) on the C++ "
                        f"oracle (assembly + imposition on {os.cpu_count()} threads) with SuperLU (sequential, "
                        f"nested-dissection order) standing in for UMFPACK; Newton iterations {newton}, LU "
-                       f"{t_lu:.1f} s of {secs:.1f} s. The bench mesh (64^3, 823,875 DOF) is out of reach of a "
+                       f"{t_lu:.1f} s of {secs:.1f} s. The bench mesh ({bench_mesh}) is out of reach of a "
                        f"direct LU in the budget (factorisation time grows ~N^2: 1.0 / 3.4 s at 16^3 / 20^3)"),
             "mesh": f"{n_cpu}^3", "newton_iters": newton, "seconds": secs, "lu_seconds": t_lu,
             "lscpu": lscpu_summary()}
@@ -249,13 +266,12 @@ def cpu_baseline(n_cpu, first, last, tol):
 
 def reference_arm(args, config):
     """`--impl reference`: timed whole increments of the CPU restatement of the reference."""
-    from plasticity_b200 import workloads as W
     n_cpu = args.cpu_n
-    nsteps = W.config2(n=n_cpu).nsteps
+    nsteps = make_workload(args.workload, n_cpu).nsteps
     first = args.warmup + 1
     last = min(args.warmup + args.steps, nsteps)
     t_all = time.perf_counter()
-    w, out, t_lu = cpu_reference(n_cpu, range(1, last + 1), 1e-10)
+    w, out, t_lu = cpu_reference(n_cpu, range(1, last + 1), 1e-10, kind=args.workload)
     timed = out[first - 1:]
     secs = sum(t for _, t in timed)
     value = len(timed) / secs
@@ -282,7 +298,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--workload", default="compress", choices=WORKLOADS,
+                    help="compress: 64^3 jittered cube, 20%% compression (the headline); indent: 150^3 "
+                         "jittered cube, central top-face indentation (10.3 M DOF)")
+    ap.add_argument("--n", type=int, default=None, help="elements per edge (default 64 / 150)")
     ap.add_argument("--cpu-n", type=int, default=16, help="mesh of the CPU baseline (elements per edge)")
     ap.add_argument("--cpu-increments", type=int, default=2)
     ap.add_argument("--no-compare", action="store_true")
@@ -295,13 +314,22 @@ def main():
     reps = Replicas("nccl")
     rank, world, local = reps.rank, reps.world, reps.local
 
-    from plasticity_b200 import workloads as W
-    w = W.config2(n=args.n)
+    if args.n is None:
+        args.n = 64 if args.workload == "compress" else 150
+    w = make_workload(args.workload, args.n)
     w.tol = args.tol
     nsteps_needed = args.warmup + args.steps
     assert nsteps_needed <= w.nsteps, f"warmup + steps must be <= {w.nsteps} increments"
-    config = {"workload": f"{w.name}: unit cube {args.n}^3 Hex8 F-bar, interior nodes jittered +-10% h, "
-                          f"lognormal sigma_y (CoV 0.1), top uz -20% in {w.nsteps} increments, bottom uz=0 + 3-2-1",
+    if args.workload == "compress":
+        desc = (f"{w.name}: unit cube {args.n}^3 Hex8 F-bar, interior nodes jittered +-10% h, lognormal sigma_y "
+                f"(CoV 0.1), top uz -20% in {w.nsteps} increments, bottom uz=0 + 3-2-1")
+    else:
+        # the FP64 comparison arms take minutes per increment-window at 10.3 M DOF
+        args.no_compare = True
+        desc = (f"{w.name}: unit cube {args.n}^3 Hex8 F-bar, interior nodes jittered +-10% h, lognormal sigma_y "
+                f"(CoV 0.1), central {w.meta['patch']}x{w.meta['patch']}-node top-face patch uz -10% in "
+                f"{w.nsteps} increments, bottom clamped; comparison arms not run at this size")
+    config = {"workload": desc,
               "elements": w.mesh.nelem, "dofs": 3 * w.mesh.nnodes, "newton_tol": w.tol,
               "timed_increments": f"{args.warmup + 1}..{nsteps_needed} of {w.nsteps}",
               "l2": "working set > 126 MB L2 (tangent alone > 250 MB); no flush",
@@ -408,7 +436,9 @@ def main():
     # ---- CPU baseline: whole increments of the reference algorithm on the oracle ----
     cpu = None
     if rank == 0 and world == 1:
-        cpu = guarded("cpu_baseline", lambda: cpu_baseline(args.cpu_n, 1, args.cpu_increments, args.tol))
+        cpu = guarded("cpu_baseline", lambda: cpu_baseline(
+            args.cpu_n, 1, args.cpu_increments, args.tol, kind=args.workload,
+            bench_mesh=f"{args.n}^3, {3 * w.mesh.nnodes:,} DOF"))
 
     # ---- side arms on the same increments ----
     out_extra = {}
