@@ -13,7 +13,14 @@ default), sets a displacement that drives most Gauss points plastic (uniform
      tolerance 1e-4, the device-side CG graph) on the imposed mixed-precision
      tangent at that displacement,
   6. `reps` single applications of the preconditioner (one V-cycle on level 0,
-     W below) outside the graph, so a launch list shows its kernels one by one.
+     W below where a level lies between level 0 and the dense coarse solve)
+     outside the graph, so a launch list shows its kernels one by one,
+  7. the imposed residual (assembly + Dirichlet imposition kernels) `reps` times,
+  8. `reps` BiCGStab solves (host-driven loop: the Krylov vector and dot kernels
+     run as separate launches, visible to a profiler),
+  9. the predictor network's loss and gradient (the backward pass) `reps` times,
+  10. four load increments (rows are recorded from the third on), then `reps`
+     training steps (backward pass + Adam update) on the recorded rows.
 
 Each family is timed with CUDA events on the library's stream and printed as one
 JSON line, so the same command serves a launch list, a single-kernel capture
@@ -80,6 +87,31 @@ def main():
     for _ in range(args.reps):
         M.amg_apply(-R)
     out["amg_cycle_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        M.residual(0.05, precision="mixed")
+    out["residual_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    _, R = M.residual(0.05, precision="mixed")
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        _, its_b = M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed", linsolve="bicgstab")
+    out["bicgstab_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    out["bicgstab_iters"] = its_b
+    T = 0.1 * rng.standard_normal((M.nn, 3)).astype(np.float32)
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        M.mlp_loss_grad(F, T)
+    out["mlp_backward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    # training rows: four converged increments from U = 0 (rows are recorded from the third on)
+    M.reset()
+    M.mlp_record("start", 4 * M.nn)
+    for s in (1, 2, 3, 4):
+        M.newton(s / w.nsteps, tol=1e-8, maxiter=40, precision="mixed", predictor="extrapolate", line_search=True)
+    out["recorded_rows"] = M.mlp_record("size")
+    M.mlp_record("stop")
+    t0 = time.perf_counter()
+    M.mlp_train(args.reps, batch=65536, lr=1e-3)
+    out["mlp_train_step_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
     print(json.dumps(out), flush=True)
 
 

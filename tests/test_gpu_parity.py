@@ -236,3 +236,70 @@ def test_write_vtu_from_gpu_model(tmp_path):
     sig = P.gauss_stress(M).T.reshape(M.ne, 8, 6).mean(axis=1)
     assert np.allclose(arrs["Stress"].reshape(M.ne, 6), sig, rtol=1e-15, atol=0)
     assert np.allclose(arrs["Displacement"], M.U, rtol=0, atol=0)
+
+
+def _check_prefix_state(M, g, label):
+    """State after increment g["last"] against a prefix fixture: U (FP64) within
+    1e-8 relative, Cauchy stress and alpha (stored in FP32) within 1e-6 of their
+    maxima, flags bit-exact."""
+    st = M.state()
+    assert rel(st["U"], g["U"]) < 1e-8, label
+    sig = P.gauss_stress(M).T
+    assert np.abs(sig - g["sigma"]).max() / np.abs(g["sigma"]).max() < 1e-6, label
+    a = st["alpha"]
+    assert np.abs(a - g["alpha"]).max() / max(np.abs(g["alpha"]).max(), 1e-300) < 1e-6, label
+    flags = np.unpackbits(g["flags_bits"])[: int(g["ngp"])]
+    assert np.array_equal(st["flags"], flags), (label, int((st["flags"] != flags).sum()))
+
+
+def _prefix_pair(w, g, precision):
+    """Increments 1..last of a load path: Newton counts of the reference's algorithm
+    (FP64, previous-U predictor, near-exact BiCGStab inner solves) within +-1 of the
+    oracle's LU-based counts, then the state at Newton tolerance 1e-10."""
+    last = int(g["last"])
+    if precision == "fp64":
+        M = model_from(w)
+        its = []
+        for s in range(1, last + 1):
+            h, _ = M.newton(s / w.nsteps, tol=float(g["tol"]), maxiter=25, linsolve="bicgstab", lin_rtol=1e-12,
+                            cg_itmax=1000)
+            its.append(len(h))
+        assert np.abs(np.array(its) - g["iters"]).max() <= 1, (its, list(g["iters"]))
+    M = model_from(w)
+    for s in range(1, last + 1):
+        M.newton(s / w.nsteps, tol=1e-10, maxiter=40, precision=precision, line_search=True,
+                 predictor="previous" if precision == "fp64" else "extrapolate",
+                 lin_rtol=1e-12 if precision == "fp64" else None)
+    _check_prefix_state(M, g, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_jittered_compression_cube16_vs_golden(precision):
+    """The bench workload's generator at 16^3 (14,739 DOF): all 40 increments of the
+    20 % compression against the oracle's LU-based solve."""
+    g = np.load(os.path.join(GOLD, "cube16_jitter_compress.npz"))
+    _prefix_pair(W.config2(n=16), g, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gathered_assembly_matches_colored(precision, monkeypatch):
+    """The row-owned gather (one element launch + one gather) and the colored
+    in-place scatter assemble the same K and R (up to summation order) on a
+    jittered mesh, and the same stress and flags."""
+    w = W.config2(n=6)
+    X = w.mesh.nodes
+    U = np.stack([0.004 * X[0], 0.002 * X[1], -0.012 * X[2]]).T.reshape(-1)
+    U += 2e-4 * np.random.default_rng(2).standard_normal(U.shape)
+    out = []
+    for mode in ("gathered", "colored"):
+        if mode == "colored":
+            monkeypatch.setenv("PFEM_ASSEMBLY", "colored")
+        M = model_from(w)
+        M.assemble(0.5 * U, commit=True)
+        out.append(M.assemble(U, precision=precision))
+        monkeypatch.delenv("PFEM_ASSEMBLY", raising=False)
+    (Kg, Rg, tg, fg), (Kc, Rc, tc, fc) = out
+    tolk = 1e-12 if precision == "fp64" else 1e-6
+    assert abs(Kg - Kc).max() <= tolk * abs(Kc).max()
+    assert np.linalg.norm(Rg - Rc) <= 1e-13 * np.linalg.norm(Rc)
+    assert np.array_equal(tg, tc) and np.array_equal(fg, fc)
