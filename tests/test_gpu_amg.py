@@ -43,12 +43,19 @@ def test_cycle_contracts():
     assert rho < 0.8, rho  # a broken cycle gives rho >= 1
 
 
+@pytest.mark.parametrize("n,its_max", [(40, 30), (80, 45)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_cg_iterations_three_levels(precision):
-    """40^3 cube: levels 0-2 plus the dense coarse solve, so the W branch below
-    level 0 runs; CG reaches 1e-6 (FP64) / 1e-5 (FP32, near its rounding floor
-    on this operator) in a bounded number of iterations."""
-    M, R = _model(40, precision)
+def test_cg_iterations_bounded(precision, n, its_max):
+    """The hierarchy stops at the first level with at most 3,600 unknowns and
+    inverts it densely.  40^3: levels 0-1 and the dense solve on level 2 (570
+    unknowns).  80^3 (1.6 M DOF): levels 0-2 and the dense solve on level 3, so
+    the W branch on level 2 runs.  CG reaches 1e-6 (FP64) / 1e-5 (FP32, near its
+    rounding floor on this operator) in a bounded number of iterations."""
+    M, R = _model(n, precision)
     x, its = M.linear_solve(-R, rtol=1e-6 if precision == "fp64" else 1e-5, rebuild=True, precision=precision)
-    assert its <= 30, its
+    assert its <= its_max, its
     assert np.all(np.isfinite(x))
+    if n == 80:
+        with pytest.raises(P.PfemError):
+            M.amg_dense(4, 0)      # levels 0..2 plus the dense level 3: no level 4
+        assert M.amg_dense(3, 0).shape[0] <= 3600 < M.amg_dense(2, 0).shape[0]
