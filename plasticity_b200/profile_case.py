@@ -28,6 +28,7 @@ JSON line, so the same command serves a launch list, a single-kernel capture
 quick timing.
 
     python -m plasticity_b200.profile_case --n 64 --reps 3
+    python -m plasticity_b200.profile_case --n 64 --reps 2 --what mlp,backward,train
 """
 from __future__ import annotations
 
@@ -38,12 +39,22 @@ import time
 import numpy as np
 
 
+FAMILIES = ("assembly", "spmv", "mlp", "amg", "residual", "bicgstab", "backward", "train")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--strain", type=float, default=0.01)
+    ap.add_argument("--what", default="all",
+                    help="comma-separated subset of " + ",".join(FAMILIES) + " (a profiler capture of one "
+                         "kernel then runs few other launches before it)")
     args = ap.parse_args()
+    what = set(FAMILIES) if args.what == "all" else set(args.what.split(","))
+    bad = what - set(FAMILIES)
+    if bad:
+        raise SystemExit(f"unknown families {sorted(bad)}")
 
     from . import model as P
     from . import predictor as PR
@@ -59,59 +70,70 @@ def main():
     M.set_displacement(U)
 
     out = {"n": args.n, "elements": w.mesh.nelem, "dofs": 3 * w.mesh.nnodes, "reps": args.reps}
-    out["assembly_mixed_ms"] = M.profile(1, reps=args.reps)
-    out["assembly_fp64_ms"] = M.profile(0, reps=args.reps)
-    out["spmv_fp32_ms"] = M.profile(2, reps=args.reps)
-    if PR.weights_available():
-        PR.load_into(M)
-    else:
-        M.mlp_init(0)
+    if "assembly" in what:
+        out["assembly_mixed_ms"] = M.profile(1, reps=args.reps)
+        out["assembly_fp64_ms"] = M.profile(0, reps=args.reps)
+    if "spmv" in what:
+        out["spmv_fp32_ms"] = M.profile(2, reps=args.reps)
     F = rng.standard_normal((M.nn, 12)).astype(np.float32)
-    M.mlp_forward(F)
-    t0 = time.perf_counter()
-    for _ in range(args.reps):
+    if what & {"mlp", "backward", "train"}:
+        if PR.weights_available():
+            PR.load_into(M)
+        else:
+            M.mlp_init(0)
+    if "mlp" in what:
         M.mlp_forward(F)
-    out["mlp_forward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
-    _, R = M.residual(0.05, precision="mixed")
-    M.linear_solve(-R, rtol=1e-4, rebuild=True, precision="mixed")  # symbolic hierarchy, once
-    t0 = time.perf_counter()
-    x, its = M.linear_solve(-R, rtol=1e-4, rebuild=True, precision="mixed")
-    out["amg_setup_and_solve_ms"] = (time.perf_counter() - t0) * 1e3
-    out["cg_iters"] = its
-    t0 = time.perf_counter()
-    for _ in range(args.reps):
-        M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed")
-    out["cg_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
-    M.amg_apply(-R)
-    t0 = time.perf_counter()
-    for _ in range(args.reps):
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            M.mlp_forward(F)
+        out["mlp_forward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    if what & {"amg", "bicgstab"}:
+        _, R = M.residual(0.05, precision="mixed")
+        M.linear_solve(-R, rtol=1e-4, rebuild=True, precision="mixed")  # symbolic hierarchy, once
+    if "amg" in what:
+        t0 = time.perf_counter()
+        x, its = M.linear_solve(-R, rtol=1e-4, rebuild=True, precision="mixed")
+        out["amg_setup_and_solve_ms"] = (time.perf_counter() - t0) * 1e3
+        out["cg_iters"] = its
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed")
+        out["cg_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
         M.amg_apply(-R)
-    out["amg_cycle_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
-    t0 = time.perf_counter()
-    for _ in range(args.reps):
-        M.residual(0.05, precision="mixed")
-    out["residual_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
-    _, R = M.residual(0.05, precision="mixed")
-    t0 = time.perf_counter()
-    for _ in range(args.reps):
-        _, its_b = M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed", linsolve="bicgstab")
-    out["bicgstab_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
-    out["bicgstab_iters"] = its_b
-    T = 0.1 * rng.standard_normal((M.nn, 3)).astype(np.float32)
-    t0 = time.perf_counter()
-    for _ in range(args.reps):
-        M.mlp_loss_grad(F, T)
-    out["mlp_backward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
-    # training rows: four converged increments from U = 0 (rows are recorded from the third on)
-    M.reset()
-    M.mlp_record("start", 4 * M.nn)
-    for s in (1, 2, 3, 4):
-        M.newton(s / w.nsteps, tol=1e-8, maxiter=40, precision="mixed", predictor="extrapolate", line_search=True)
-    out["recorded_rows"] = M.mlp_record("size")
-    M.mlp_record("stop")
-    t0 = time.perf_counter()
-    M.mlp_train(args.reps, batch=65536, lr=1e-3)
-    out["mlp_train_step_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            M.amg_apply(-R)
+        out["amg_cycle_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    if "residual" in what:
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            M.residual(0.05, precision="mixed")
+        out["residual_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    if "bicgstab" in what:
+        _, R = M.residual(0.05, precision="mixed")
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            _, its_b = M.linear_solve(-R, rtol=1e-4, rebuild=False, precision="mixed", linsolve="bicgstab")
+        out["bicgstab_solve_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+        out["bicgstab_iters"] = its_b
+    if "backward" in what:
+        T = 0.1 * rng.standard_normal((M.nn, 3)).astype(np.float32)
+        t0 = time.perf_counter()
+        for _ in range(args.reps):
+            M.mlp_loss_grad(F, T)
+        out["mlp_backward_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+    if "train" in what:
+        # training rows: four converged increments from U = 0 (rows are recorded from the third on)
+        M.reset()
+        M.mlp_record("start", 4 * M.nn)
+        for s in (1, 2, 3, 4):
+            M.newton(s / w.nsteps, tol=1e-8, maxiter=40, precision="mixed", predictor="extrapolate",
+                     line_search=True)
+        out["recorded_rows"] = M.mlp_record("size")
+        M.mlp_record("stop")
+        t0 = time.perf_counter()
+        M.mlp_train(args.reps, batch=65536, lr=1e-3)
+        out["mlp_train_step_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
     print(json.dumps(out), flush=True)
 
 
