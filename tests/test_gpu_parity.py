@@ -274,6 +274,15 @@ def _prefix_pair(w, g, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_necking_bar_full_size_vs_golden(precision):
+    """Configuration 1 at its stated size (80 x 16 x 16 Hex8, 70,227 DOF; sigma_y -2 %
+    in the middle element layer, 30 % stretch in 60 increments), the first 15
+    increments, against the oracle's LU-based solve."""
+    g = np.load(os.path.join(GOLD, "bar80x16x16_neck_15.npz"))
+    _prefix_pair(W.config1(), g, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_jittered_compression_cube16_vs_golden(precision):
     """The bench workload's generator at 16^3 (14,739 DOF): all 40 increments of the
     20 % compression against the oracle's LU-based solve."""
