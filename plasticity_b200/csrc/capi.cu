@@ -449,6 +449,11 @@ void mgs_qr(int m, std::vector<double>& A, double R[36]) {
 // matrix-vector product per cycle.  At 64^3 this is level 2 (512 aggregates,
 // 3,072 unknowns): one product in place of a W-cycle's two visits to it.
 constexpr long long kCoarseDenseMax = 3600;
+// Coarsest levels up to this size are inverted on the host with partial pivoting
+// (n^3 <= 2e8 flops); larger ones on the device without row exchanges, which the
+// coarse operators of large meshes (full aggregates, every rigid mode present)
+// do not need.
+constexpr int kCoarseHostMax = 600;
 
 void build_amg_structure(pfem_ctx* c) {
   c->hl.clear();
@@ -699,6 +704,42 @@ int krylov_alloc(pfem_ctx* ctx) {
   return PFEM_OK;
 }
 
+// Gauss-Jordan inverse of a dense n x n matrix (row-major, double) with
+// partial pivoting; near-singular pivots are regularised.  Used for small
+// coarsest levels (at most kCoarseHostMax unknowns), where a pivot-free
+// elimination can meet tiny pivots: partially constrained aggregates leave
+// coarse rows that are nearly dependent.
+void dense_inverse_host(int n, std::vector<double>& a, std::vector<double>& inv) {
+  inv.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+  double scl = 0;
+  for (int i = 0; i < n; ++i) scl = std::max(scl, std::fabs(a[(size_t)i * n + i]));
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    double best = std::fabs(a[(size_t)c * n + c]);
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(a[(size_t)r * n + c]) > best) { best = std::fabs(a[(size_t)r * n + c]); piv = r; }
+    if (piv != c)
+      for (int j = 0; j < n; ++j) {
+        std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
+        std::swap(inv[(size_t)c * n + j], inv[(size_t)piv * n + j]);
+      }
+    double pv = a[(size_t)c * n + c];
+    if (std::fabs(pv) < 1e-14 * std::max(scl, 1e-300)) pv = (pv >= 0 ? 1.0 : -1.0) * 1e-14 * std::max(scl, 1e-300);
+    const double ip = 1.0 / pv;
+    for (int j = 0; j < n; ++j) { a[(size_t)c * n + j] *= ip; inv[(size_t)c * n + j] *= ip; }
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      const double f = a[(size_t)r * n + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) {
+        a[(size_t)r * n + j] -= f * a[(size_t)c * n + j];
+        inv[(size_t)r * n + j] -= f * inv[(size_t)c * n + j];
+      }
+    }
+  }
+}
+
 // Numeric AMG set-up on the current (Dirichlet-imposed) tangent of precision T:
 // block-Jacobi inverses, Chebyshev bounds by power iteration, Galerkin
 // coarse operators, dense coarse inverse -- all on the device.  Rebuilt per load step by default
@@ -744,10 +785,36 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     sa_setup_level<T>(v, omega, cval, nnzC, ctx->st);
     CKL();
   }
-  // coarsest operator: dense inverse on the device (at most kCoarseDenseMax unknowns)
-  pfem::dense_coarse_inverse<T>(ctx->hl[L].nbrow, A.coarse_rp, A.coarse_cl, A.coarse_val, A.coarse_n,
-                                ctx->dDenseWork, A.coarse_inv, ctx->st);
-  CKL();
+  // coarsest operator: dense inverse, on the device (blocked Gauss-Jordan) for
+  // large coarsest levels, on the host with partial pivoting for small ones
+  if (A.coarse_n > kCoarseHostMax) {
+    pfem::dense_coarse_inverse<T>(ctx->hl[L].nbrow, A.coarse_rp, A.coarse_cl, A.coarse_val, A.coarse_n,
+                                  ctx->dDenseWork, A.coarse_inv, ctx->st);
+    CKL();
+  } else {
+    const HostLevel& hc = ctx->hl[L];
+    std::vector<T> hv((size_t)A.coarse_nnzb * 36);
+    CK(cudaMemcpyAsync(hv.data(), A.coarse_val, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const int n = A.coarse_n;
+    std::vector<double> dense((size_t)n * n, 0.0), inv;
+    for (int I = 0; I < hc.nbrow; ++I)
+      for (int k = hc.rowptr[I]; k < hc.rowptr[I + 1]; ++k) {
+        const int J = hc.col[k];
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 6; ++c) dense[(size_t)(I * 6 + r) * n + J * 6 + c] = (double)hv[(size_t)k * 36 + r * 6 + c];
+      }
+    // rigid modes absent from an aggregate leave zero rows: put 1 on their diagonal
+    for (int i = 0; i < n; ++i) {
+      bool zero = true;
+      for (int j = 0; j < n && zero; ++j) zero = dense[(size_t)i * n + j] == 0.0;
+      if (zero) dense[(size_t)i * n + i] = 1.0;
+    }
+    dense_inverse_host(n, dense, inv);
+    std::vector<T> invT(inv.begin(), inv.end());
+    CK(cudaMemcpyAsync(A.coarse_inv, invT.data(), invT.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
   A.built = true;
   A.version++;
   return PFEM_OK;
