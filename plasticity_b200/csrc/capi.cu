@@ -1283,14 +1283,23 @@ int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool
       rc = amg_setup<double>(ctx, o->cheb_degree);
       if (rc) return rc;
     } else {
-      ctx->amg64.lv[0].A.val = ctx->dK64;
+      // reused hierarchy: the level-0 operator is the current tangent, and so is
+      // the block-Jacobi inverse of the level-0 smoother (one pass over the
+      // diagonal blocks); the coarse levels stay as built
+      AmgLevel<double>& v0 = ctx->amg64.lv[0];
+      v0.A.val = ctx->dK64;
+      blockdiag_invert<double>(v0.A, v0.dinv, ctx->st);
+      CKL();
     }
   } else {
     if (rebuild || !ctx->amg32.built) {
       rc = amg_setup<float>(ctx, o->cheb_degree);
       if (rc) return rc;
     } else {
-      ctx->amg32.lv[0].A.val = ctx->dK32;
+      AmgLevel<float>& v0 = ctx->amg32.lv[0];
+      v0.A.val = ctx->dK32;
+      blockdiag_invert<float>(v0.A, v0.dinv, ctx->st);
+      CKL();
     }
   }
   CK(cudaStreamSynchronize(ctx->st));
