@@ -211,14 +211,16 @@ def test_reused_model_takes_new_boundary_values():
 
 
 def test_load_step_cutting_recovers_a_failed_increment():
-    """10 % compression per increment fails (the reference stops); with max_cuts the
-    failed increments are retried at half size and the path completes."""
+    """10 % compression per increment under the reference's plain Newton (no line
+    search) inverts an element and the reference stops (the oracle's exact-LU Newton
+    inverts element 4 on the first increment); with max_cuts the failed increment is
+    retried at half size and the path completes (the oracle needs one cut)."""
     w = W.config2(n=4, nsteps=2)
     M = model_from(w)
-    plain = M.solve(nsteps=2, tol=1e-8, maxiter=25, line_search=True)
+    plain = M.solve(nsteps=2, tol=1e-8, maxiter=25)
     assert not plain.converged
     M = model_from(w)
-    cut = M.solve(nsteps=2, tol=1e-8, maxiter=25, line_search=True, max_cuts=8)
+    cut = M.solve(nsteps=2, tol=1e-8, maxiter=25, max_cuts=8)
     assert cut.converged and cut.stats["load_step_cuts"] > 0, cut.stats
     assert len(cut.iters) == 2
 
