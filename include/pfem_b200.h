@@ -199,13 +199,16 @@ int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, in
                       const pfem_solve_opts* o, int32_t* niter);
 
 /* One cycle of the AMG hierarchy last built by pfem_linear_solve / Newton
- * (precision of the resident tangent; a V on the finest level, a W below
- * it): z = M^-1 r, host vectors of ndof. */
+ * (precision of the resident tangent; a V on the finest level, a W on the
+ * levels between it and the dense coarsest level): z = M^-1 r, host vectors
+ * of ndof. */
 int pfem_amg_apply(pfem_ctx* ctx, const double* r, double* z);
 
 /* Inspection of the resident AMG hierarchy (small problems): the dense
- * operator of `level` (what = 0, n_l x n_l, row-major) or its smoothed
- * prolongator (what = 1, n_l x n_{l+1}); dims receives (rows, cols). */
+ * operator of `level` (what = 0, n_l x n_l, row-major), its smoothed
+ * prolongator (what = 1, n_l x n_{l+1}), or, for the coarsest level L, the
+ * dense inverse the cycle applies (what = 2, n_L x n_L); dims receives
+ * (rows, cols). */
 int pfem_amg_dense(pfem_ctx* ctx, int32_t level, int32_t what, double* out, int64_t* dims);
 
 /* Read-out: nodal_displacements / gauss_kirchhoff / equivalent_plastic_strain /

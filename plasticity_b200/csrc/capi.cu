@@ -1496,10 +1496,20 @@ template <typename T>
 static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t* dims) {
   Amg<T>& A = amg_of<T>(ctx);
   const int L = (int)A.lv.size();
-  if (!A.built || level < 0 || level > L || (what == 1 && level >= L))
+  if (!A.built || level < 0 || level > L || (what == 1 && level >= L) || (what == 2 && level != L) || what < 0 ||
+      what > 2)
     return fail(ctx, PFEM_ERR_BAD_ARG, "no such AMG level");
   const HostLevel& h = ctx->hl[level];
   const int bs = h.bs, nr = h.nbrow * bs;
+  if (what == 2) {  // the dense inverse of the coarsest level, as the cycle applies it
+    const int n = A.coarse_n;
+    if (dims) { dims[0] = n; dims[1] = n; }
+    if (!out) return PFEM_OK;
+    std::vector<T> v((size_t)n * n);
+    CK(cudaMemcpy(v.data(), A.coarse_inv, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < v.size(); ++i) out[i] = (double)v[i];
+    return PFEM_OK;
+  }
   if (what == 0) {
     if (dims) { dims[0] = nr; dims[1] = nr; }
     if (!out) return PFEM_OK;

@@ -5,20 +5,20 @@
 // Solver.jl:136-154).  The coarsest operator (6 x 6 blocks, a few thousand
 // unknowns) is expanded to a dense FP64 matrix and inverted in place by blocked
 // Gauss-Jordan elimination; the cycle then applies the inverse as one dense
-// matrix-vector product.  Per panel of NB columns:
-//   1. panel kernel: every CTA inverts the NB x NB diagonal block in shared
-//      memory (the same arithmetic in every CTA, so all copies agree; the first
-//      one stores it in Dg), scales the panel rows outside the diagonal block by
-//      it, and saves the old panel columns of the other rows in C;
-//   2. update kernel: A[i, j] -= C[i, :] P[:, j] for every row i outside the
-//      panel (P the scaled panel rows, Dg in the panel's own columns), with the
-//      panel's own columns starting from 0, which turns them into -C D^{-1};
-//      the diagonal block becomes Dg.
-// The diagonal block of A is read by every panel CTA and written only by the
-// update kernel, so no CTA can see it half replaced.
-// No row exchanges: the Galerkin operator of the (Dirichlet-imposed) tangent is
-// close to symmetric positive definite; a pivot below 1e-14 of the largest
-// diagonal entry is replaced by that floor, as the host inverse did before.
+// matrix-vector product.  Per panel of NB columns K:
+//   1. diagonal kernel (one CTA): Dg = A[K,K]^{-1} by Gauss-Jordan in shared memory;
+//   2. panel kernel: the panel rows outside the diagonal block, A[K,j] <- Dg A[K,j],
+//      and a copy C = A[i,K] of the panel columns of the other rows;
+//   3. update kernel: A[i, j] -= C[i, :] P[:, j] for every row i outside the panel
+//      (P the scaled panel rows, Dg in the panel's own columns), with the panel's
+//      own columns starting from 0, which turns them into -C Dg; the tile that
+//      holds the diagonal block writes Dg there.
+// Every kernel reads only what the previous one finished writing, and A[K,K] is
+// read only by the diagonal kernel, so no CTA sees a block half replaced.
+// No row exchanges: the Galerkin operator of the (Dirichlet-imposed) tangent of a
+// large mesh is close to symmetric positive definite (small coarsest levels are
+// inverted on the host with partial pivoting instead); a pivot below 1e-14 of the
+// largest diagonal entry is replaced by that floor.
 #include <cstdint>
 
 #include "linalg.cuh"
@@ -26,8 +26,9 @@
 namespace pfem {
 namespace {
 
-constexpr int NB = 32;      // panel width
-constexpr int TILE = 64;    // update tile (rows and columns)
+constexpr int NB = 64;      // panel width
+constexpr int TR_ = 128;    // update tile rows
+constexpr int TC_ = 64;     // update tile columns
 
 // Dense row-major n x n FP64 matrix from the coarsest level's 6 x 6 blocks.
 template <typename T>
@@ -76,9 +77,14 @@ __global__ void dense_diag_max_kernel(int n, const double* __restrict__ A, doubl
   }
 }
 
-// In-place Gauss-Jordan inverse of the NB x NB block M (shared memory), 256 threads.
-__device__ void invert_block(double (*M)[NB + 1], double floor_abs) {
+// Dg = A[K,K]^{-1}: in-place Gauss-Jordan on the NB x NB diagonal block in
+// shared memory, one CTA of 1024 threads (four entries each).
+__global__ void __launch_bounds__(1024) gj_diag_kernel(int n, int kb, const double* __restrict__ A,
+                                                       double* __restrict__ Dg, const double* __restrict__ scl) {
+  __shared__ double M[NB][NB + 1];
   const int t = threadIdx.x;
+  for (int e = t; e < NB * NB; e += 1024) M[e / NB][e % NB] = A[(long long)(kb + e / NB) * n + kb + e % NB];
+  const double floor_abs = 1e-14 * fmax(scl[0], 1e-300);
   for (int k = 0; k < NB; ++k) {
     __syncthreads();
     double piv = M[k][k];
@@ -87,12 +93,11 @@ __device__ void invert_block(double (*M)[NB + 1], double floor_abs) {
     __syncthreads();
     if (t < NB) M[k][t] = (t == k ? 1.0 : M[k][t]) * ip;
     __syncthreads();
-    // each thread owns 4 entries of rows i != k
     double f[4];
     int ii[4], jj[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = t + q * 256;
+      const int e = t + q * 1024;
       ii[q] = e / NB;
       jj[q] = e % NB;
       f[q] = M[ii[q]][k];
@@ -106,88 +111,102 @@ __device__ void invert_block(double (*M)[NB + 1], double floor_abs) {
     }
   }
   __syncthreads();
+  for (int e = t; e < NB * NB; e += 1024) Dg[e] = M[e / NB][e % NB];
 }
 
-// Panel step kb: CTAs [0, ncb) scale the panel rows (256 columns each),
-// CTAs [ncb, ncb + nrb) save the panel columns of 256 rows each into C (n x NB).
+// Panel step kb.  CTAs [0, ncb): 64 panel-row columns each, A[K, j] <- Dg A[K, j]
+// for j outside K (the 64 x 64 slab staged in shared memory; thread (column,
+// quarter) computes 16 rows).  CTAs [ncb, ...): C[i, :] = A[i, K] for rows i
+// outside K, a warp per row.
 __global__ void __launch_bounds__(256) gj_panel_kernel(int n, int kb, int ncb, double* __restrict__ A,
-                                                       double* __restrict__ C, double* __restrict__ Dg,
-                                                       const double* __restrict__ scl) {
-  __shared__ double D[NB][NB + 1];
+                                                       double* __restrict__ C, const double* __restrict__ Dg) {
+  extern __shared__ __align__(16) double psm[];
   const int t = threadIdx.x;
   if ((int)blockIdx.x >= ncb) {
-    const int i = ((int)blockIdx.x - ncb) * 256 + t;
+    const int w = t >> 5, lane = t & 31;
+    const int i = ((int)blockIdx.x - ncb) * 8 + w;
     if (i < n && (i < kb || i >= kb + NB)) {
-#pragma unroll 8
-      for (int s = 0; s < NB; ++s) C[(long long)i * NB + s] = A[(long long)i * n + kb + s];
+      C[(long long)i * NB + lane] = A[(long long)i * n + kb + lane];
+      C[(long long)i * NB + 32 + lane] = A[(long long)i * n + kb + 32 + lane];
     }
     return;
   }
-  for (int e = t; e < NB * NB; e += 256) D[e / NB][e % NB] = A[(long long)(kb + e / NB) * n + kb + e % NB];
-  invert_block(D, 1e-14 * fmax(scl[0], 1e-300));
-  if (blockIdx.x == 0)
-    for (int e = t; e < NB * NB; e += 256) Dg[e] = D[e / NB][e % NB];
-  const int j = (int)blockIdx.x * 256 + t;
-  if (j >= n || (j >= kb && j < kb + NB)) return;
-  double v[NB];
-#pragma unroll
-  for (int s = 0; s < NB; ++s) v[s] = A[(long long)(kb + s) * n + j];
-#pragma unroll 4
-  for (int r = 0; r < NB; ++r) {
-    double acc = 0.0;
-#pragma unroll
-    for (int s = 0; s < NB; ++s) acc += D[r][s] * v[s];
-    A[(long long)(kb + r) * n + j] = acc;
+  const int j0 = (int)blockIdx.x * 64;
+  if (j0 == kb) return;  // the diagonal block's columns: Dg, written by the update kernel
+  double(*D)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm);
+  double(*V)[65] = reinterpret_cast<double(*)[65]>(psm + NB * (NB + 1));
+  for (int e = t; e < NB * NB; e += 256) D[e / NB][e % NB] = Dg[e];
+  for (int e = t; e < NB * 64; e += 256) {
+    const int r = e / 64, c = e % 64, j = j0 + c;
+    V[r][c] = j < n ? A[(long long)(kb + r) * n + j] : 0.0;
   }
+  __syncthreads();
+  const int c = t & 63, q = t >> 6, j = j0 + c;
+  if (j >= n) return;
+  double out[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) out[r] = 0.0;
+#pragma unroll 8
+  for (int s = 0; s < NB; ++s) {
+    const double v = V[s][c];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) out[r] += D[q * 16 + r][s] * v;
+  }
+#pragma unroll
+  for (int r = 0; r < 16; ++r) A[(long long)(kb + q * 16 + r) * n + j] = out[r];
 }
 
-// Trailing update of step kb over TILE x TILE tiles; rows of the panel are final.
-__global__ void __launch_bounds__(256) gj_update_kernel(int n, int kb, double* __restrict__ A,
-                                                        const double* __restrict__ C, const double* __restrict__ Dg) {
-  __shared__ double Cs[TILE][NB + 1];
-  __shared__ double Ps[NB][TILE + 1];
-  const int i0 = (int)blockIdx.y * TILE, j0 = (int)blockIdx.x * TILE;
+// Trailing update of step kb over TR_ x TC_ tiles; rows of the panel are final.
+// Thread (rg, cg) holds rows rg*8 .. +7 and columns cg + 16 b, b < 4.
+__global__ void __launch_bounds__(256, 2) gj_update_kernel(int n, int kb, double* __restrict__ A,
+                                                           const double* __restrict__ C,
+                                                           const double* __restrict__ Dg) {
+  extern __shared__ __align__(16) double usm[];
+  double(*Cs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(usm);              // TR_ x NB
+  double(*Ps)[TC_ + 1] = reinterpret_cast<double(*)[TC_ + 1]>(usm + TR_ * (NB + 1));  // NB x TC_
+  const int i0 = (int)blockIdx.y * TR_, j0 = (int)blockIdx.x * TC_;
   const int t = threadIdx.x;
-  for (int e = t; e < TILE * NB; e += 256) {
+  for (int e = t; e < TR_ * NB; e += 256) {
     const int r = e / NB, s = e % NB, i = i0 + r;
     Cs[r][s] = (i < n && (i < kb || i >= kb + NB)) ? C[(long long)i * NB + s] : 0.0;
   }
-  for (int e = t; e < NB * TILE; e += 256) {
-    const int s = e / TILE, c = e % TILE, j = j0 + c;
-    Ps[s][c] = j >= n ? 0.0 : (j >= kb && j < kb + NB) ? Dg[s * NB + (j - kb)] : A[(long long)(kb + s) * n + j];
+  const bool diag_cols = j0 == kb;  // TC_ == NB and both are multiples of NB: the panel is one column tile
+  for (int e = t; e < NB * TC_; e += 256) {
+    const int s = e / TC_, c = e % TC_, j = j0 + c;
+    Ps[s][c] = j >= n ? 0.0 : diag_cols ? Dg[s * NB + c] : A[(long long)(kb + s) * n + j];
   }
   // the tile holding the diagonal block writes it (no other CTA reads it from A)
-  if (kb >= i0 && kb < i0 + TILE && kb >= j0 && kb < j0 + TILE)
+  if (diag_cols && kb >= i0 && kb < i0 + TR_)
     for (int e = t; e < NB * NB; e += 256) A[(long long)(kb + e / NB) * n + kb + e % NB] = Dg[e];
   __syncthreads();
-  const int rg = t / 16, cg = t % 16;  // rows rg*4 .. +3, columns cg + 16 b
-  double acc[4][4];
+  const int rg = t / 16, cg = t % 16;
+  double acc[8][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-#pragma unroll 8
+#pragma unroll 4
   for (int s = 0; s < NB; ++s) {
-    double cv[4], pv[4];
+    double cv[8], pv[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) cv[a] = Cs[rg * 4 + a][s];
+    for (int a = 0; a < 8; ++a) cv[a] = Cs[rg * 8 + a][s];
 #pragma unroll
     for (int b = 0; b < 4; ++b) pv[b] = Ps[s][cg + 16 * b];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 8; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] += cv[a] * pv[b];
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = i0 + rg * 4 + a;
+  for (int a = 0; a < 8; ++a) {
+    const int i = i0 + rg * 8 + a;
     if (i >= n || (i >= kb && i < kb + NB)) continue;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
       const int j = j0 + cg + 16 * b;
       if (j >= n) continue;
       double* p = A + (long long)i * n + j;
-      const double old = (j >= kb && j < kb + NB) ? 0.0 : *p;
+      const double old = diag_cols ? 0.0 : *p;
       *p = old - acc[a][b];
     }
   }
@@ -220,6 +239,14 @@ void dense_coarse_inverse(int nbrow, const int* rp, const int* cl, const T* val,
   double* C = work + (long long)np * np;
   double* Dg = C + (long long)np * NB;
   double* scl = Dg + NB * NB;
+  const size_t panel_sm = (size_t)(NB * (NB + 1) + NB * 65) * sizeof(double);
+  const size_t update_sm = (size_t)(TR_ * (NB + 1) + NB * (TC_ + 1)) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(gj_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_sm);
+    cudaFuncSetAttribute(gj_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)update_sm);
+    attr = true;
+  }
   cudaMemsetAsync(A, 0, (size_t)np * np * sizeof(double), st);
   count_launch();
   bsr6_to_dense_kernel<T><<<1024, 256, 0, st>>>(nbrow, rp, cl, val, np, A);
@@ -227,13 +254,15 @@ void dense_coarse_inverse(int nbrow, const int* rp, const int* cl, const T* val,
   dense_fix_rows_kernel<<<(np + 7) / 8, 256, 0, st>>>(np, A);
   count_launch();
   dense_diag_max_kernel<<<1, 1024, 0, st>>>(np, A, scl);
-  const int ncb = (np + 255) / 256, nrb = (np + 255) / 256;
-  const dim3 ug((np + TILE - 1) / TILE, (np + TILE - 1) / TILE);
+  const int ncb = np / 64, nrb = (np + 7) / 8;
+  const dim3 ug((np + TC_ - 1) / TC_, (np + TR_ - 1) / TR_);
   for (int kb = 0; kb < np; kb += NB) {
     count_launch();
-    gj_panel_kernel<<<ncb + nrb, 256, 0, st>>>(np, kb, ncb, A, C, Dg, scl);
+    gj_diag_kernel<<<1, 1024, 0, st>>>(np, kb, A, Dg, scl);
     count_launch();
-    gj_update_kernel<<<ug, 256, 0, st>>>(np, kb, A, C, Dg);
+    gj_panel_kernel<<<ncb + nrb, 256, panel_sm, st>>>(np, kb, ncb, A, C, Dg);
+    count_launch();
+    gj_update_kernel<<<ug, 256, update_sm, st>>>(np, kb, A, C, Dg);
   }
   count_launch();
   dense_out_kernel<T><<<2048, 256, 0, st>>>(n, np, A, inv);

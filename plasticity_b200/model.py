@@ -382,7 +382,8 @@ class Model:
         return z
 
     def amg_dense(self, level, what):
-        """Dense copy of an AMG operator (what=0) or prolongator (what=1)."""
+        """Dense copy of an AMG operator (what=0), prolongator (what=1) or, on the
+        coarsest level, the dense inverse the cycle applies (what=2)."""
         dims = np.zeros(2, np.int64)
         check(L.lib().pfem_amg_dense(self._ctx, level, what, None, ptr(dims, L._i64)), self._ctx)
         out = np.zeros((int(dims[0]), int(dims[1])))

@@ -59,3 +59,26 @@ def test_cg_iterations_bounded(precision, n, its_max):
         with pytest.raises(P.PfemError):
             M.amg_dense(4, 0)      # levels 0..2 plus the dense level 3: no level 4
         assert M.amg_dense(3, 0).shape[0] <= 3600 < M.amg_dense(2, 0).shape[0]
+
+
+@pytest.mark.parametrize("n,device_path", [(10, False), (48, True)])
+def test_coarse_dense_inverse(n, device_path):
+    """The coarsest level's dense inverse: on the host with partial pivoting up to
+    600 unknowns (10^3: level 1), on the device by blocked Gauss-Jordan above
+    (48^3: level 2, about 1,300 unknowns); either way inverse times operator is the
+    identity to rounding."""
+    M, R = _model(n, "fp64")
+    M.linear_solve(-R, rtol=1e-8, rebuild=True, precision="fp64")
+    for L in range(1, 6):        # only the coarsest level answers what = 2
+        try:
+            Ai = M.amg_dense(L, 2)
+            break
+        except P.PfemError:
+            continue
+    Ac = M.amg_dense(L, 0)
+    assert (Ac.shape[0] > 600) == device_path, Ac.shape
+    # rows of rigid modes absent from an aggregate are empty; both inverses give
+    # them a unit diagonal, so compare on the others
+    nz = np.abs(Ac).sum(axis=1) > 0
+    E = (Ai @ Ac)[np.ix_(nz, nz)] - np.eye(int(nz.sum()))
+    assert np.abs(E).max() < 1e-8, np.abs(E).max()
