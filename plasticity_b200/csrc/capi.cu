@@ -1324,23 +1324,17 @@ int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool
       rc = amg_setup<double>(ctx, o->cheb_degree);
       if (rc) return rc;
     } else {
-      // reused hierarchy: the level-0 operator is the current tangent, and so is
-      // the block-Jacobi inverse of the level-0 smoother (one pass over the
-      // diagonal blocks); the coarse levels stay as built
-      AmgLevel<double>& v0 = ctx->amg64.lv[0];
-      v0.A.val = ctx->dK64;
-      blockdiag_invert<double>(v0.A, v0.dinv, ctx->st);
-      CKL();
+      // reused hierarchy: the level-0 operator is the current tangent; the
+      // smoother keeps the block-Jacobi inverse its Chebyshev interval was
+      // estimated with (a fresh inverse under the old interval can diverge)
+      ctx->amg64.lv[0].A.val = ctx->dK64;
     }
   } else {
     if (rebuild || !ctx->amg32.built) {
       rc = amg_setup<float>(ctx, o->cheb_degree);
       if (rc) return rc;
     } else {
-      AmgLevel<float>& v0 = ctx->amg32.lv[0];
-      v0.A.val = ctx->dK32;
-      blockdiag_invert<float>(v0.A, v0.dinv, ctx->st);
-      CKL();
+      ctx->amg32.lv[0].A.val = ctx->dK32;
     }
   }
   CK(cudaStreamSynchronize(ctx->st));

@@ -1075,10 +1075,7 @@ void launch_element_color(const ElemArgs<KT>& a, const int* elist, int n, bool c
 // One warp per node a: the row's blocks accumulate in shared memory, element by
 // element in increasing element order (a fixed order: deterministic sums).
 // Within one element the 72 values go to 72 distinct entries (eight distinct
-// column nodes), so the lanes never add into the same entry at once.  The loads
-// of up to eight incident elements (element ids, positions, rank bytes, values,
-// forces) are all issued before the first add, so a node waits for one memory
-// latency rather than one per element.
+// column nodes), so the lanes never add into the same entry at once.
 template <typename KT>
 __global__ void __launch_bounds__(256) gather_rows_kernel(int nn, const int* __restrict__ nptr,
                                                           const int* __restrict__ nel,
@@ -1088,7 +1085,6 @@ __global__ void __launch_bounds__(256) gather_rows_kernel(int nn, const int* __r
                                                           const KT* __restrict__ Kbuf,
                                                           const double* __restrict__ Fbuf, KT* __restrict__ Kval,
                                                           double* __restrict__ R, int maxlen) {
-  constexpr int QB = 8;  // elements loaded per batch (a hex-mesh node has at most 8)
   extern __shared__ __align__(16) unsigned char gsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = (int)blockIdx.x * (int)(blockDim.x >> 5) + warp;
@@ -1097,54 +1093,19 @@ __global__ void __launch_bounds__(256) gather_rows_kernel(int nn, const int* __r
   const int r0 = browptr[a], len9 = (browptr[a + 1] - r0) * 9;
   for (int v = lane; v < len9; v += 32) acc[v] = KT(0);
   double fr = 0.0;
-  // this lane's three value slots v = lane, lane + 32, lane + 64 (v < 72) of an
-  // element's 72: row i = v / 24, column (b, k) = v % 24
-  int vb[3], voff[3];
-#pragma unroll
-  for (int u = 0; u < 3; ++u) {
-    const int v = lane + 32 * u, i = v / 24, col = v - 24 * i, b = col / 3, k = col - 3 * b;
-    vb[u] = b;
-    voff[u] = i * 3 + k;
-  }
-  const int q0 = nptr[a], nq = nptr[a + 1] - q0;
-  for (int base = 0; base < nq; base += QB) {
-    const int cnt = min(QB, nq - base);
-    int e_l = 0, al_l = 0;
-    if (lane < cnt) {
-      e_l = nel[q0 + base + lane];
-      al_l = nloc[q0 + base + lane];
+  __syncwarp();
+  const int q1 = nptr[a + 1];
+  for (int q = nptr[a]; q < q1; ++q) {
+    const int e = nel[q];
+    const int al = nloc[q];
+    const KT* src = Kbuf + (long long)e * 576 + al * 72;
+    const uint8_t* rk = rank + (long long)e * 64 + al * 8;
+    for (int v = lane; v < 72; v += 32) {
+      const int i = v / 24, col = v - 24 * i, b = col / 3, k = col - 3 * b;
+      acc[rk[b] * 9 + i * 3 + k] += __ldcs(src + v);
     }
-    KT val[QB][3];
-    int pos[QB][3];
-    double f[QB];
-#pragma unroll
-    for (int j = 0; j < QB; ++j) {
-      const int e = __shfl_sync(0xffffffffu, e_l, j), al = __shfl_sync(0xffffffffu, al_l, j);
-      f[j] = 0.0;
-#pragma unroll
-      for (int u = 0; u < 3; ++u) { val[j][u] = KT(0); pos[j][u] = 0; }
-      if (j < cnt) {
-        const KT* src = Kbuf + (long long)e * 576 + al * 72;
-        const uint8_t* rk = rank + (long long)e * 64 + al * 8;
-#pragma unroll
-        for (int u = 0; u < 3; ++u)
-          if (lane + 32 * u < 72) {
-            val[j][u] = __ldcs(src + lane + 32 * u);
-            pos[j][u] = rk[vb[u]] * 9 + voff[u];
-          }
-        if (lane < 3) f[j] = Fbuf[(long long)e * 24 + al * 3 + lane];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < QB; ++j) {
-      if (j < cnt) {
-#pragma unroll
-        for (int u = 0; u < 3; ++u)
-          if (lane + 32 * u < 72) acc[pos[j][u]] += val[j][u];
-        fr += f[j];
-      }
-      __syncwarp();
-    }
+    if (lane < 3) fr += Fbuf[(long long)e * 24 + al * 3 + lane];
+    __syncwarp();
   }
   KT* dst = Kval + (long long)r0 * 9;
   for (int v = lane; v < len9; v += 32) dst[v] = acc[v];

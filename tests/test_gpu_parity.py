@@ -211,18 +211,19 @@ def test_reused_model_takes_new_boundary_values():
 
 
 def test_load_step_cutting_recovers_a_failed_increment():
-    """10 % compression per increment under the reference's plain Newton (no line
-    search) inverts an element and the reference stops (the oracle's exact-LU Newton
-    inverts element 4 on the first increment); with max_cuts the failed increment is
-    retried at half size and the path completes (the oracle needs one cut)."""
-    w = W.config2(n=4, nsteps=2)
+    """30 % compression in one increment moves the top nodes of the 4-element-high
+    cube further than an element is tall, so the reference's plain Newton inverts
+    an element on its first iterate and stops (the oracle does the same); with
+    max_cuts the increment is retried at half size until it converges and then
+    carried on to the full load (the oracle needs four cuts)."""
+    w = W.config2(n=4, nsteps=1, compress=0.3)
     M = model_from(w)
-    plain = M.solve(nsteps=2, tol=1e-8, maxiter=25)
+    plain = M.solve(nsteps=1, tol=1e-8, maxiter=25)
     assert not plain.converged
     M = model_from(w)
-    cut = M.solve(nsteps=2, tol=1e-8, maxiter=25, max_cuts=8)
+    cut = M.solve(nsteps=1, tol=1e-8, maxiter=25, max_cuts=8)
     assert cut.converged and cut.stats["load_step_cuts"] > 0, cut.stats
-    assert len(cut.iters) == 2
+    assert len(cut.iters) == 1
 
 
 def test_write_vtu_from_gpu_model(tmp_path):
