@@ -1112,6 +1112,68 @@ __global__ void __launch_bounds__(256) gather_rows_kernel(int nn, const int* __r
   if (lane < 3) R[(long long)a * 3 + lane] = fr;
 }
 
+// Rows of at most 32 blocks (every hex mesh: 27): lane p of the node's warp owns
+// block p of the row in registers.  The node's element ids, positions and rank
+// bytes are loaded once, one element per lane; then, element by element in
+// increasing order, the lane whose position appears among the element's eight
+// rank bytes (at most one does, per column node b) adds that 3 x 3 block.  The
+// value loads of different elements do not depend on each other, nothing goes
+// through shared memory, and each lane sums in the same element order as the
+// shared-memory gather above.
+template <typename KT>
+__global__ void __launch_bounds__(256) gather_rows_lane_kernel(int nn, const int* __restrict__ nptr,
+                                                               const int* __restrict__ nel,
+                                                               const uint8_t* __restrict__ nloc,
+                                                               const int* __restrict__ browptr,
+                                                               const uint8_t* __restrict__ rank,
+                                                               const KT* __restrict__ Kbuf,
+                                                               const double* __restrict__ Fbuf,
+                                                               KT* __restrict__ Kval, double* __restrict__ R) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = (int)blockIdx.x * (int)(blockDim.x >> 5) + warp;
+  if (a >= nn) return;  // whole warps
+  const int r0 = browptr[a], len = browptr[a + 1] - r0;
+  const int q0 = nptr[a], nq = nptr[a + 1] - q0;
+  const unsigned key = (unsigned)lane * 0x01010101u;
+  KT acc[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) acc[v] = KT(0);
+  double fr = 0.0;
+  for (int base = 0; base < nq; base += 32) {
+    const int cnt = min(32, nq - base);
+    int e_l = 0, al_l = 0;
+    unsigned lo_l = 0xFFFFFFFFu, hi_l = 0xFFFFFFFFu;
+    if (lane < cnt) {
+      e_l = nel[q0 + base + lane];
+      al_l = nloc[q0 + base + lane];
+      const uint2 rk = *reinterpret_cast<const uint2*>(rank + (long long)e_l * 64 + al_l * 8);
+      lo_l = rk.x;
+      hi_l = rk.y;
+    }
+#pragma unroll 4
+    for (int j = 0; j < cnt; ++j) {
+      const int e = __shfl_sync(0xffffffffu, e_l, j), al = __shfl_sync(0xffffffffu, al_l, j);
+      const unsigned lo = __shfl_sync(0xffffffffu, lo_l, j), hi = __shfl_sync(0xffffffffu, hi_l, j);
+      const unsigned ml = __vcmpeq4(lo, key), mh = __vcmpeq4(hi, key);
+      const int b = ml ? ((__ffs(ml) - 1) >> 3) : (mh ? 4 + ((__ffs(mh) - 1) >> 3) : -1);
+      if (b >= 0) {
+        const KT* src = Kbuf + (long long)e * 576 + al * 72 + b * 3;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) acc[i * 3 + k] += __ldcs(src + i * 24 + k);
+      }
+      if (lane < 3) fr += Fbuf[(long long)e * 24 + al * 3 + lane];
+    }
+  }
+  if (lane < len) {
+    KT* dst = Kval + (long long)(r0 + lane) * 9;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) dst[v] = acc[v];
+  }
+  if (lane < 3) R[(long long)a * 3 + lane] = fr;
+}
+
 template <typename KT>
 void launch_gather_rows(int nn, const int* nptr, const int* nel, const uint8_t* nloc, const int* browptr,
                         const uint8_t* rank, const KT* Kbuf, const double* Fbuf, KT* Kval, double* R, int maxlen,
@@ -1120,6 +1182,11 @@ void launch_gather_rows(int nn, const int* nptr, const int* nel, const uint8_t* 
   const size_t sm = (size_t)WARPS * maxlen * 9 * sizeof(KT);
   const int blocks = (nn + WARPS - 1) / WARPS;
   if (blocks <= 0) return;
+  if (maxlen <= 32) {
+    pfem::count_launch();
+    gather_rows_lane_kernel<KT><<<blocks, 32 * WARPS, 0, st>>>(nn, nptr, nel, nloc, browptr, rank, Kbuf, Fbuf, Kval, R);
+    return;
+  }
   if (sm > 48 * 1024)  // rows longer than a hex mesh's 27 blocks (the 8-bit rank table caps them at 256)
     cudaFuncSetAttribute(gather_rows_kernel<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   pfem::count_launch();
