@@ -56,7 +56,6 @@ struct CgGraph {
   double* ctl = nullptr;   // device: [0] rtol, [1] itmax, [2] absolute threshold (set on the device)
   int* state = nullptr;    // device: [0] iterations, [1] converged
   long long prefix_kernels = 0, body_kernels = 0;
-  bool programmatic = false;  // the body's kernel-to-kernel edges are programmatic
 };
 
 struct HostLevel {
@@ -118,7 +117,6 @@ struct pfem_ctx {
   uint8_t* dNloc = nullptr;
   int max_row = 0;
   bool colored_assembly = false;
-  bool cg_pdl = true;  // programmatic edges in the CG loop body (cleared if the driver refuses them)
   float* dKbuf32 = nullptr;
   double* dKbuf64 = nullptr;
   double* dFbuf = nullptr;
@@ -903,7 +901,6 @@ template <typename T>
 __global__ void cg_graph_check_kernel(cudaGraphConditionalHandle h, const T* __restrict__ part, int np,
                                       T* __restrict__ sc_rn, const double* __restrict__ ctl,
                                       int* __restrict__ state) {
-  pfem::pdl_wait();
   __shared__ T sh[32];
   T v = T(0);
   for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
@@ -924,32 +921,6 @@ __global__ void cg_graph_check_kernel(cudaGraphConditionalHandle h, const T* __r
   const bool conv = r <= ctl[2];
   state[1] = conv ? 1 : 0;
   cudaGraphSetConditional(h, (!conv && isfinite(r) && it < (int)ctl[1]) ? 1u : 0u);
-}
-
-// Turn every kernel-to-kernel edge of g into a programmatic edge from the
-// launch-completion port: the downstream kernel is launched once every block of
-// the upstream one has started, and waits inside (pdl_wait) for the upstream
-// grid to complete, so its launch overlaps the upstream tail.  Every kernel of
-// the CG loop body starts with pdl_wait.  Returns false if the driver refuses.
-bool make_edges_programmatic(cudaGraph_t g) {
-  size_t ne = 0;
-  if (cudaGraphGetEdges_v2(g, nullptr, nullptr, nullptr, &ne) != cudaSuccess) return false;
-  std::vector<cudaGraphNode_t> from(ne), to(ne);
-  std::vector<cudaGraphEdgeData> ed(ne);
-  if (ne && cudaGraphGetEdges_v2(g, from.data(), to.data(), ed.data(), &ne) != cudaSuccess) return false;
-  for (size_t i = 0; i < ne; ++i) {
-    cudaGraphNodeType ta, tb;
-    if (cudaGraphNodeGetType(from[i], &ta) != cudaSuccess || cudaGraphNodeGetType(to[i], &tb) != cudaSuccess)
-      return false;
-    if (ta != cudaGraphNodeTypeKernel || tb != cudaGraphNodeTypeKernel || ed[i].type != cudaGraphDependencyTypeDefault)
-      continue;
-    cudaGraphEdgeData e2 = {};
-    e2.from_port = cudaGraphKernelNodePortLaunchCompletion;
-    e2.type = cudaGraphDependencyTypeProgrammatic;
-    if (cudaGraphRemoveDependencies_v2(g, &from[i], &to[i], &ed[i], 1) != cudaSuccess) return false;
-    if (cudaGraphAddDependencies_v2(g, &from[i], &to[i], &e2, 1) != cudaSuccess) return false;
-  }
-  return true;
 }
 
 // Capture (or reuse) the device-side CG loop for the current hierarchy.
@@ -1038,23 +1009,11 @@ int cg_graph_build(pfem_ctx* ctx) {
     return fail(ctx, PFEM_ERR_CUDA, std::string("CG graph capture (end): ") + cudaGetErrorString(e));
   }
   G.graph = g;
-  const bool pdl = ctx->cg_pdl && make_edges_programmatic(body);
   e = cudaGraphInstantiate(&G.exec, g, 0);
-  if (e != cudaSuccess && pdl) {
-    // the driver refused programmatic edges in the loop body: capture again with plain edges
-    cudaGetLastError();
-    G.exec = nullptr;
-    cudaGraphDestroy(g);
-    G.graph = nullptr;
-    pfem::launch_counter() = c0;
-    ctx->cg_pdl = false;
-    return cg_graph_build<T>(ctx);
-  }
   if (e != cudaSuccess) {
     G.exec = nullptr;
     return fail(ctx, PFEM_ERR_CUDA, std::string("CG graph instantiate: ") + cudaGetErrorString(e));
   }
-  G.programmatic = pdl;
   // launches are counted when the graph runs, not when it is captured
   G.prefix_kernels = c1 - c0 + 1;
   G.body_kernels = c2 - c1 + 1;
@@ -1858,8 +1817,6 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     for (int64_t n = 0; n < nn; ++n) ctx->max_row = std::max(ctx->max_row, ctx->browptr[n + 1] - ctx->browptr[n]);
     const char* am = getenv("PFEM_ASSEMBLY");
     ctx->colored_assembly = am && std::string(am) == "colored";
-    const char* pd = getenv("PFEM_CG_PDL");
-    ctx->cg_pdl = !(pd && std::string(pd) == "0");
   }
   if (sigy0_e) {
     std::vector<double> s(sigy0_e, sigy0_e + ne);

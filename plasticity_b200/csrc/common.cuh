@@ -25,12 +25,6 @@ long long& launch_counter();
 void set_last_error(const std::string& msg);
 inline void count_launch() { ++launch_counter(); }
 
-// First statement of every kernel that can run inside the CG loop graph, whose
-// kernel-to-kernel edges are programmatic (a kernel is launched once all blocks
-// of its predecessor have started): waits until the predecessor grid has
-// completed and its writes are visible.  Returns at once for an ordinary launch.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 // Material constants with the derived moduli of J2Material
 // (lagrangian/src/Materials.jl:104-107).
 struct MatParams {

@@ -24,7 +24,6 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
                                                        const T* __restrict__ b,
                                                        const T* __restrict__ dinv, T* __restrict__ xo,
                                                        T c1, T c2) {
-  pdl_wait();
   // Half a warp per block row (a level-0 row has at most 27 blocks: two per
   // lane); values and column ids are read once, through the streaming
   // (evict-first) path so they do not push the gathered x out of the caches.
@@ -156,7 +155,6 @@ void bsr_residual_precond(const BsrMat<T>& A, const T* dinv, const T* x, const T
 template <typename T, int BS>
 __global__ void blockdiag_apply_kernel(int nbrow, const T* __restrict__ dinv, const T* __restrict__ v,
                                        T* __restrict__ r, T scale, T* __restrict__ d) {
-  pdl_wait();
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)nbrow * BS) return;
   const long long row = i / BS;
@@ -256,7 +254,6 @@ __device__ __forceinline__ T block_sum(T v, T* sh) {
 template <typename T>
 __global__ void dot_partial_kernel(long long n, const T* __restrict__ a, const T* __restrict__ b,
                                    T* __restrict__ part) {
-  pdl_wait();
   __shared__ T sh[32];
   T v = T(0);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -267,7 +264,6 @@ __global__ void dot_partial_kernel(long long n, const T* __restrict__ a, const T
 }
 template <typename T>
 __global__ void sum_final_kernel(int np, const T* __restrict__ part, T* __restrict__ out, int sqrt_out) {
-  pdl_wait();
   __shared__ T sh[32];
   T v = T(0);
   for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
@@ -285,7 +281,6 @@ void dot(long long n, const T* a, const T* b, T* out, T* part, cudaStream_t st, 
 // ------------------------------------------------------------------ vector ops
 template <typename T>
 __global__ void fill_kernel(long long n, T* x, T v) {
-  pdl_wait();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     x[i] = v;
 }
@@ -297,7 +292,6 @@ void fill(long long n, T* x, T v, cudaStream_t st) {
 // y = a*x + b*y with host scalars
 template <typename T>
 __global__ void axpby_kernel(long long n, T a, const T* __restrict__ x, T b, T* __restrict__ y) {
-  pdl_wait();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = a * x[i] + b * y[i];
 }
@@ -311,7 +305,6 @@ template <typename T>
 __global__ void cg_xr_kernel(long long n, const T* __restrict__ num, const T* __restrict__ den,
                              const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
                              T* __restrict__ r) {
-  pdl_wait();
   const T al = *num / *den;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     x[i] += al * p[i];
@@ -327,7 +320,6 @@ void cg_xr(long long n, const T* num, const T* den, const T* p, const T* q, T* x
 template <typename T>
 __global__ void cg_p_kernel(long long n, const T* __restrict__ num, const T* __restrict__ den,
                             const T* __restrict__ z, T* __restrict__ p) {
-  pdl_wait();
   const T be = *num / *den;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     p[i] = z[i] + be * p[i];
@@ -354,7 +346,6 @@ __device__ __forceinline__ T all_sum_partials(const T* __restrict__ part, int np
 template <typename T>
 __global__ void cg_p_fused_kernel(long long n, const T* __restrict__ part, int np, T* __restrict__ sc,
                                   const T* __restrict__ z, T* __restrict__ p) {
-  pdl_wait();
   __shared__ T sh[33];
   const T rz = all_sum_partials(part, np, sh);
   const T be = rz / sc[0];
@@ -368,7 +359,6 @@ template <typename T>
 __global__ void cg_xr_fused_kernel(long long n, const T* __restrict__ part_pq, int np, T* __restrict__ sc,
                                    const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ x,
                                    T* __restrict__ r, T* __restrict__ part_rr) {
-  pdl_wait();
   __shared__ T sh[33];
   const T pq = all_sum_partials(part_pq, np, sh);
   const T al = sc[2] / pq;
@@ -412,7 +402,6 @@ int cg_xr_fused(long long n, const T* part_pq, int np, T* sc, const T* p, const 
 template <typename T>
 __global__ void bicg_p_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ r,
                               const T* __restrict__ v, T* __restrict__ p) {
-  pdl_wait();
   // beta = (rho_new/rho_old)*(alpha/omega); p = r + beta (p - omega v)
   const T beta = (sc[0] / sc[1]) * (sc[2] / sc[3]);
   const T om = sc[3];
@@ -428,7 +417,6 @@ void bicg_p(long long n, const T* sc, const T* r, const T* v, T* p, cudaStream_t
 template <typename T>
 __global__ void bicg_s_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ r,
                               const T* __restrict__ v, T* __restrict__ s) {
-  pdl_wait();
   const T al = sc[0] / sc[4];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     s[i] = r[i] - al * v[i];
@@ -443,7 +431,6 @@ template <typename T>
 __global__ void bicg_xr_kernel(long long n, const T* __restrict__ sc, const T* __restrict__ ph,
                                const T* __restrict__ sh, const T* __restrict__ s, const T* __restrict__ t,
                                T* __restrict__ x, T* __restrict__ r) {
-  pdl_wait();
   const T al = sc[0] / sc[4];
   const T om = sc[5] / sc[6];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -459,10 +446,7 @@ void bicg_xr(long long n, const T* sc, const T* ph, const T* sh, const T* s, con
 }
 // scalar bookkeeping: dst[i] = src[j]
 template <typename T>
-__global__ void scalar_copy_kernel(T* dst, const T* src) {
-  pdl_wait();
-  *dst = *src;
-}
+__global__ void scalar_copy_kernel(T* dst, const T* src) { *dst = *src; }
 template <typename T>
 void scalar_copy(T* dst, const T* src, cudaStream_t st) {
   pfem::count_launch();
@@ -472,7 +456,6 @@ void scalar_copy(T* dst, const T* src, cudaStream_t st) {
 // precision conversion
 template <typename A, typename B>
 __global__ void convert_kernel(long long n, const A* __restrict__ a, B* __restrict__ b, double s) {
-  pdl_wait();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     b[i] = (B)(s * (double)a[i]);
 }
@@ -568,7 +551,6 @@ void bc_apply(const BcDev& bc, double lam, double* U, cudaStream_t st) {
 // Dense coarse solve y = Ainv b (one warp per row).
 template <typename T>
 __global__ void dense_mv_kernel(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ y) {
-  pdl_wait();
   const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
@@ -733,7 +715,6 @@ __global__ void sa_transpose_copy_kernel(int nnzP, const int* __restrict__ pt_bl
 template <typename T, int BS>
 __global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, const int* __restrict__ pt_row,
                                    const T* __restrict__ ptval, const T* __restrict__ r, T* __restrict__ bc) {
-  pdl_wait();
   const int I = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (I >= nagg) return;  // whole warps exit together
@@ -763,7 +744,6 @@ __global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, cons
 template <typename T, int BS>
 __global__ void sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp, const int* __restrict__ p_cl,
                                   const T* __restrict__ pval, const T* __restrict__ xc, T* __restrict__ x) {
-  pdl_wait();
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)nbrow * BS) return;
   const int n = (int)(i / BS), j = (int)(i % BS);
