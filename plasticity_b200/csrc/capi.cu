@@ -142,6 +142,8 @@ struct pfem_ctx {
   // first solve after the last rebuild, and whether a later solve exceeded it
   double amg_ipd_base = -1.0;
   bool amg_stale = true;
+  double amg_excess = 0.0;      // Krylov iterations above the fresh rate since the last rebuild
+  double amg_cost_iters = 0.0;  // the last rebuild's time in Krylov iterations of its hierarchy
   double lam_prev = 0.0, lam_prev2 = 0.0, lam_prev3 = 0.0;
 };
 
@@ -445,10 +447,13 @@ void mgs_qr(int m, std::vector<double>& A, double R[36]) {
 // of the Galerkin operator P^T A P of every level.  Level 0 uses the
 // tangent's block pattern in place (its rowptr/col stay empty).
 // The hierarchy stops at the first level with at most this many unknowns; that
-// level is inverted densely on the device (dense.cu) and applied as one dense
-// matrix-vector product per cycle.  At 64^3 this is level 2 (512 aggregates,
-// 3,072 unknowns): one product in place of a W-cycle's two visits to it.
-constexpr long long kCoarseDenseMax = 3600;
+// level is inverted densely (dense.cu on the device, or on the host when small)
+// and applied as one dense matrix-vector product per cycle.  The inverse costs
+// n^3 at every rebuild: at 64^3 a 3,072-unknown dense level 2 saves a W-cycle's
+// two visits to it (about 100 us per cycle) but adds about 11 ms per rebuild,
+// so by default the hierarchy goes one level further there (162 unknowns).
+// PFEM_COARSE_DENSE_MAX overrides the bound.
+constexpr long long kCoarseDenseMax = 1500;
 // Coarsest levels up to this size are inverted on the host with partial pivoting
 // (n^3 <= 2e8 flops); larger ones on the device without row exchanges, which the
 // coarse operators of large meshes (full aggregates, every rigid mode present)
@@ -456,6 +461,8 @@ constexpr long long kCoarseDenseMax = 3600;
 constexpr int kCoarseHostMax = 600;
 
 void build_amg_structure(pfem_ctx* c) {
+  long long dense_max = kCoarseDenseMax;
+  if (const char* e = getenv("PFEM_COARSE_DENSE_MAX")) dense_max = std::max(1LL, atoll(e));
   c->hl.clear();
   HostLevel cur;
   cur.nbrow = (int)c->nn;
@@ -467,7 +474,7 @@ void build_amg_structure(pfem_ctx* c) {
   bool first = true;
   for (int lev = 0; lev < 10; ++lev) {
     const int nb = cur.nbrow, bs = cur.bs;
-    if ((long long)nb * bs <= kCoarseDenseMax && !first) break;
+    if ((long long)nb * bs <= dense_max && !first) break;
     const int* rp = first ? c->browptr.data() : cur.rowptr.data();
     const int* cl = first ? c->bcol.data() : cur.col.data();
     const int* grp = first ? rp : cur.grp.data();
@@ -1375,6 +1382,7 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     first = false;
     int kits = 0;
     bool kconv = true;
+    double amg0 = tm->amg_ms, kry0 = tm->kry_ms;
     rc = newton_correction(ctx, o, eta, rebuild, &kits, &tm->amg_ms, &tm->kry_ms, &kconv);
     if (rc) return rc;
     if (o->amg_rebuild == 2 && !rebuild && !kconv) {
@@ -1382,17 +1390,30 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
       // so the adaptive policy never takes a worse direction than the per-step rebuild
       tm->kits += kits;
       rebuild = true;
+      amg0 = tm->amg_ms;
+      kry0 = tm->kry_ms;
       rc = newton_correction(ctx, o, eta, true, &kits, &tm->amg_ms, &tm->kry_ms, &kconv);
       if (rc) return rc;
     }
     if (o->amg_rebuild == 2) {
       // iterations per decade of residual reduction asked of this solve
-      const double ipd = kits / std::max(std::log10(1.0 / eta), 0.5);
+      const double dec = std::max(std::log10(1.0 / eta), 0.5);
+      const double ipd = kits / dec;
       if (rebuild) {
         ctx->amg_ipd_base = ipd;
         ctx->amg_stale = false;
-      } else if (kits > o->amg_stale_ratio * ctx->amg_ipd_base * std::max(std::log10(1.0 / eta), 0.5) + 2) {
-        ctx->amg_stale = true;
+        ctx->amg_excess = 0.0;
+        // what a rebuild costs, in Krylov iterations on the fresh hierarchy
+        const double t_it = kits > 0 ? (tm->kry_ms - kry0) / kits : 0.0;
+        ctx->amg_cost_iters = t_it > 0.0 ? (tm->amg_ms - amg0) / t_it : 0.0;
+      } else {
+        // stale when one solve needs amg_stale_ratio times the fresh rate, or when the
+        // iterations spent above the fresh rate since the rebuild have cost more than
+        // a rebuild would have
+        const double expect = ctx->amg_ipd_base * dec;
+        ctx->amg_excess += std::max(0.0, kits - expect);
+        if (kits > o->amg_stale_ratio * expect + 2 || ctx->amg_excess > ctx->amg_cost_iters)
+          ctx->amg_stale = true;
       }
     }
     if (khist) khist[it - 1] = kits;

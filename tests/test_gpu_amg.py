@@ -46,7 +46,7 @@ def test_cycle_contracts():
 @pytest.mark.parametrize("n,its_max", [(40, 30), (80, 45)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_cg_iterations_bounded(precision, n, its_max):
-    """The hierarchy stops at the first level with at most 3,600 unknowns and
+    """The hierarchy stops at the first level with at most 1,500 unknowns and
     inverts it densely.  40^3: levels 0-1 and the dense solve on level 2 (570
     unknowns).  80^3 (1.6 M DOF): levels 0-2 and the dense solve on level 3, so
     the W branch on level 2 runs.  CG reaches 1e-6 (FP64) / 1e-5 (FP32, near its
@@ -58,7 +58,7 @@ def test_cg_iterations_bounded(precision, n, its_max):
     if n == 80:
         with pytest.raises(P.PfemError):
             M.amg_dense(4, 0)      # levels 0..2 plus the dense level 3: no level 4
-        assert M.amg_dense(3, 0).shape[0] <= 3600 < M.amg_dense(2, 0).shape[0]
+        assert M.amg_dense(3, 0).shape[0] <= 1500 < M.amg_dense(2, 0).shape[0]
 
 
 @pytest.mark.parametrize("n,device_path", [(10, False), (48, True)])
