@@ -654,6 +654,7 @@ int amg_alloc(pfem_ctx* ctx) {
     if (l == 0) {
       v.A.rowptr = ctx->dBrowptr;
       v.A.col = ctx->dBcol;
+      v.A.maxrow = ctx->max_row;
     } else {
       CK(upload(ctx, &v.A.rowptr, h.rowptr));
       CK(upload(ctx, &v.A.col, h.col));
@@ -2391,6 +2392,9 @@ int pfem_solve(pfem_ctx* ctx, const pfem_solve_opts* o, pfem_solve_result* res, 
       CK(cudaMemcpyAsync(ctx->dU, ctx->dUprev, ctx->ndof * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st));
       lam = ctx->lam_prev + 0.5 * (lam - ctx->lam_prev);
       ctx->err.clear();
+      // the hierarchy was built on the abandoned attempt's iterates (possibly next to an
+      // inverted element): the retry starts from a hierarchy of the converged state
+      ctx->amg_stale = true;
     }
     if (r.converged) r.steps_done = n;
   }

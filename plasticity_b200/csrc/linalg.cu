@@ -16,29 +16,62 @@ namespace pfem {
 //   0: y = A x
 //   1: y = b - A x                          (residual)
 //   2: r -= Dinv (A x); xo += x             (Chebyshev step on x = d)
-template <typename T, int BS, int MODE, bool VEC = false>
+// Staged variant (STAGED, rows of at most STAGE_BLOCKS blocks): the half-warp
+// first copies its row's contiguous value segment into shared memory with
+// 16-byte streaming loads from the aligned address at or below the segment's
+// start, so every load instruction reads 256 consecutive bytes; the lanes then
+// take their blocks from shared memory (a stride of 9 words: no bank conflicts).
+constexpr int STAGE_BLOCKS = 32;
+
+template <typename T, int BS, int MODE, bool VEC = false, bool STAGED = false>
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __restrict__ rowptr,
                                                        const int* __restrict__ col,
                                                        const T* __restrict__ val,
                                                        const T* __restrict__ x, T* __restrict__ y,
                                                        const T* __restrict__ b,
                                                        const T* __restrict__ dinv, T* __restrict__ xo,
-                                                       T c1, T c2) {
+                                                       T c1, T c2, long long nval) {
   // Half a warp per block row (a level-0 row has at most 27 blocks: two per
   // lane); values and column ids are read once, through the streaming
   // (evict-first) path so they do not push the gathered x out of the caches.
+  constexpr int PER = 16 / (int)sizeof(T);
+  constexpr int STAGE = STAGED ? STAGE_BLOCKS * BS * BS + PER : 1;
+  __shared__ __align__(16) T stage_sm[STAGED ? 16 : 1][STAGE];
   const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4);
   const int lane = threadIdx.x & 15;
   const bool ok = row < nbrow;
   const int s = ok ? rowptr[row] : 0, e = ok ? rowptr[row + 1] : 0;
+  int off = 0;
+  if constexpr (STAGED) {
+    using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
+    T* st = stage_sm[threadIdx.x >> 4];
+    const long long vs = (long long)s * (BS * BS), ve = (long long)e * (BS * BS);
+    const long long a0 = vs & ~(long long)(PER - 1);
+    const int nvec = (int)((ve - a0 + PER - 1) / PER);
+    for (int j = lane; j < nvec; j += 16) {
+      const long long g = a0 + (long long)j * PER;
+      if (g + PER <= nval) {
+        const V v = __ldcs(reinterpret_cast<const V*>(val + g));
+        *reinterpret_cast<V*>(st + j * PER) = v;
+      } else {
+#pragma unroll
+        for (int q = 0; q < PER; ++q) st[j * PER + q] = g + q < nval ? __ldcs(val + g + q) : T(0);
+      }
+    }
+    __syncwarp();
+    off = (int)(vs - a0);
+  }
   T acc[BS];
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
   for (int k = s + lane; k < e; k += 16) {
     const int c = __ldcs(col + k);
-    const T* B = val + (long long)k * (BS * BS);
+    const T* B = STAGED ? stage_sm[threadIdx.x >> 4] + off + (k - s) * (BS * BS) : val + (long long)k * (BS * BS);
     T bv[BS * BS];
-    if constexpr (VEC) {
+    if constexpr (STAGED) {
+#pragma unroll
+      for (int q = 0; q < BS * BS; ++q) bv[q] = B[q];
+    } else if constexpr (VEC) {
       // 16-byte streaming loads (a 6 x 6 block is 144 / 288 bytes; the launcher
       // checks that val is 16-byte aligned, so every block is)
       using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
@@ -116,14 +149,21 @@ static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const 
                         cudaStream_t st) {
   const long long threads = (long long)A.nbrow * 16;
   const int blocks = (int)((threads + 255) / 256);
+  const long long nval = A.nnzb * A.bs * A.bs;
+  const bool aligned = (reinterpret_cast<uintptr_t>(A.val) & 15) == 0;
   pfem::count_launch();
-  if (A.bs == 3)
-    bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
-  else if ((reinterpret_cast<uintptr_t>(A.val) & 15) == 0)
+  if (A.bs == 3 && aligned && A.maxrow > 0 && A.maxrow <= STAGE_BLOCKS)
+    bsr_spmv_kernel<T, 3, MODE, false, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv,
+                                                                     xo, c1, c2, nval);
+  else if (A.bs == 3)
+    bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2,
+                                                        nval);
+  else if (aligned)
     bsr_spmv_kernel<T, 6, MODE, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1,
-                                                              c2);
+                                                              c2, nval);
   else
-    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2,
+                                                        nval);
 }
 
 template <typename T>

@@ -70,6 +70,7 @@ struct BsrMat {
   int* rowptr = nullptr;  // device, nbrow+1
   int* col = nullptr;     // device, nnzb
   VT* val = nullptr;      // device, nnzb*bs*bs (row-major blocks)
+  int maxrow = 0;         // longest block row (0: unknown)
 };
 
 // One level of smoothed-aggregation AMG.  Every fine block row n belongs to
