@@ -654,7 +654,6 @@ int amg_alloc(pfem_ctx* ctx) {
     if (l == 0) {
       v.A.rowptr = ctx->dBrowptr;
       v.A.col = ctx->dBcol;
-      v.A.maxrow = ctx->max_row;
     } else {
       CK(upload(ctx, &v.A.rowptr, h.rowptr));
       CK(upload(ctx, &v.A.col, h.col));
@@ -683,6 +682,7 @@ int amg_alloc(pfem_ctx* ctx) {
     const size_t n = (size_t)h.nbrow * h.bs;
     CK(dalloc(ctx, &v.x, n)); CK(dalloc(ctx, &v.b, n)); CK(dalloc(ctx, &v.r, n));
     CK(dalloc(ctx, &v.d, n)); CK(dalloc(ctx, &v.t, n));
+    if (l >= 2) { CK(dalloc(ctx, &v.b2, n)); CK(dalloc(ctx, &v.x2, n)); }
   }
   const HostLevel& hc = ctx->hl[L];
   A.coarse_n = hc.nbrow * hc.bs;
@@ -880,14 +880,18 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
   sa_restrict<T>(v, v.t, bn, ctx->st);
   if (l + 1 < L) vcycle<T>(ctx, l + 1, bn, xn);
   else dense_mv<T>(A.coarse_n, A.coarse_inv, bn, xn, ctx->st);
-  sa_prolong<T>(v, xn, x, ctx->st);
   if (l >= 1 && l + 1 < L) {
-    // Below the finest level the cycle is a W: a second coarse correction
-    // from the updated residual.  The coarse levels cost a small fraction of
-    // level 0, and the stronger coarse solve cuts the outer CG iterations.
-    bsr_residual<T>(v.A, x, b, v.t, ctx->st);
-    sa_restrict<T>(v, v.t, bn, ctx->st);
-    vcycle<T>(ctx, l + 1, bn, xn);
+    // Below the finest level the cycle is a W: two iterations on the coarse
+    // problem.  The second starts from the coarse residual bn - A_c xn, which
+    // equals the restriction of the updated fine residual because A_c is the
+    // Galerkin product P^T A P, so this level's matrix is not read again; both
+    // corrections are prolonged in one pass.  The coarse levels cost a small
+    // fraction of level 0, and the stronger coarse solve cuts the CG iterations.
+    AmgLevel<T>& c = A.lv[l + 1];
+    bsr_residual<T>(c.A, xn, bn, c.b2, ctx->st);
+    vcycle<T>(ctx, l + 1, c.b2, c.x2);
+    sa_prolong2<T>(v, xn, c.x2, x, ctx->st);
+  } else {
     sa_prolong<T>(v, xn, x, ctx->st);
   }
   cheb<T>(ctx, v, A.cheb_degree, b, x, false);

@@ -10,68 +10,38 @@
 namespace pfem {
 
 // ------------------------------------------------------------------ SpMV
-// One warp per block row; lane k holds block rowptr[i]+k (+32, ...), loads the
-// whole bs x bs block and the matching bs entries of x, and the warp reduces
-// the bs partial sums.  Mode selects the epilogue:
+// Half a warp per block row; lane k holds block rowptr[i]+k (+16, ...), loads
+// the whole bs x bs block and the matching bs entries of x, and the half-warp
+// reduces the bs partial sums by a fixed xor tree.  Mode selects the epilogue:
 //   0: y = A x
 //   1: y = b - A x                          (residual)
 //   2: r -= Dinv (A x); xo += x             (Chebyshev step on x = d)
-// Staged variant (STAGED, rows of at most STAGE_BLOCKS blocks): the half-warp
-// first copies its row's contiguous value segment into shared memory with
-// 16-byte streaming loads from the aligned address at or below the segment's
-// start, so every load instruction reads 256 consecutive bytes; the lanes then
-// take their blocks from shared memory (a stride of 9 words: no bank conflicts).
-constexpr int STAGE_BLOCKS = 32;
-
-template <typename T, int BS, int MODE, bool VEC = false, bool STAGED = false>
+//   3: xo = c2 x + c1 (y - Dinv A x)        (fused degree-2 Chebyshev, x = d0, y = r0)
+//   4: as 3, added to xo
+//   5: y = Dinv (b - A x), xo = c1 y        (preconditioned residual + first direction)
+template <typename T, int BS, int MODE, bool VEC = false>
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __restrict__ rowptr,
                                                        const int* __restrict__ col,
                                                        const T* __restrict__ val,
                                                        const T* __restrict__ x, T* __restrict__ y,
                                                        const T* __restrict__ b,
                                                        const T* __restrict__ dinv, T* __restrict__ xo,
-                                                       T c1, T c2, long long nval) {
+                                                       T c1, T c2) {
   // Half a warp per block row (a level-0 row has at most 27 blocks: two per
   // lane); values and column ids are read once, through the streaming
   // (evict-first) path so they do not push the gathered x out of the caches.
-  constexpr int PER = 16 / (int)sizeof(T);
-  constexpr int STAGE = STAGED ? STAGE_BLOCKS * BS * BS + PER : 1;
-  __shared__ __align__(16) T stage_sm[STAGED ? 16 : 1][STAGE];
   const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4);
   const int lane = threadIdx.x & 15;
   const bool ok = row < nbrow;
   const int s = ok ? rowptr[row] : 0, e = ok ? rowptr[row + 1] : 0;
-  int off = 0;
-  if constexpr (STAGED) {
-    using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
-    T* st = stage_sm[threadIdx.x >> 4];
-    const long long vs = (long long)s * (BS * BS), ve = (long long)e * (BS * BS);
-    const long long a0 = vs & ~(long long)(PER - 1);
-    const int nvec = (int)((ve - a0 + PER - 1) / PER);
-    for (int j = lane; j < nvec; j += 16) {
-      const long long g = a0 + (long long)j * PER;
-      if (g + PER <= nval) {
-        const V v = __ldcs(reinterpret_cast<const V*>(val + g));
-        *reinterpret_cast<V*>(st + j * PER) = v;
-      } else {
-#pragma unroll
-        for (int q = 0; q < PER; ++q) st[j * PER + q] = g + q < nval ? __ldcs(val + g + q) : T(0);
-      }
-    }
-    __syncwarp();
-    off = (int)(vs - a0);
-  }
   T acc[BS];
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
   for (int k = s + lane; k < e; k += 16) {
     const int c = __ldcs(col + k);
-    const T* B = STAGED ? stage_sm[threadIdx.x >> 4] + off + (k - s) * (BS * BS) : val + (long long)k * (BS * BS);
+    const T* B = val + (long long)k * (BS * BS);
     T bv[BS * BS];
-    if constexpr (STAGED) {
-#pragma unroll
-      for (int q = 0; q < BS * BS; ++q) bv[q] = B[q];
-    } else if constexpr (VEC) {
+    if constexpr (VEC) {
       // 16-byte streaming loads (a 6 x 6 block is 144 / 288 bytes; the launcher
       // checks that val is 16-byte aligned, so every block is)
       using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
@@ -149,21 +119,14 @@ static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const 
                         cudaStream_t st) {
   const long long threads = (long long)A.nbrow * 16;
   const int blocks = (int)((threads + 255) / 256);
-  const long long nval = A.nnzb * A.bs * A.bs;
-  const bool aligned = (reinterpret_cast<uintptr_t>(A.val) & 15) == 0;
   pfem::count_launch();
-  if (A.bs == 3 && aligned && A.maxrow > 0 && A.maxrow <= STAGE_BLOCKS)
-    bsr_spmv_kernel<T, 3, MODE, false, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv,
-                                                                     xo, c1, c2, nval);
-  else if (A.bs == 3)
-    bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2,
-                                                        nval);
-  else if (aligned)
+  if (A.bs == 3)
+    bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+  else if ((reinterpret_cast<uintptr_t>(A.val) & 15) == 0)
     bsr_spmv_kernel<T, 6, MODE, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1,
-                                                              c2, nval);
+                                                              c2);
   else
-    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2,
-                                                        nval);
+    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
 }
 
 template <typename T>
@@ -748,26 +711,77 @@ __global__ void sa_transpose_copy_kernel(int nnzP, const int* __restrict__ pt_bl
   ptval[e] = pval[(long long)pt_blk[t] * (BS * 6) + q];
 }
 
-// Restriction bc = P^T r, one warp per aggregate: the lanes stride over the
-// aggregate's P blocks in the P^T-ordered copy (consecutive lanes read
-// consecutive blocks) and the six partial sums are combined by a fixed xor
-// tree, so the result is deterministic.
+// Transfer kernels stage the P values they stream in shared memory: a warp copies
+// CB blocks at a time with coalesced 16-byte streaming loads (from the aligned
+// address at or below the chunk's first value; the chunk's values are
+// contiguous), then its lanes take their blocks from shared memory.
 template <typename T, int BS>
-__global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, const int* __restrict__ pt_row,
-                                   const T* __restrict__ ptval, const T* __restrict__ r, T* __restrict__ bc) {
-  const int I = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
+struct TransferCfg {
+  static constexpr int PER = 16 / (int)sizeof(T);
+  static constexpr int BV = BS * 6;  // values of one bs x 6 block
+  static constexpr int CB = BV * (int)sizeof(T) * 32 * 8 <= 40 * 1024 ? 32 : 16;  // blocks per chunk
+  static constexpr int STAGE = CB * BV + PER;
+  static_assert(CB * BV % PER == 0, "chunks end on 16-byte groups");
+};
+
+// Copy blocks [tb, tb + nb) of vals (nval values in all) into st; returns the
+// offset of block tb's first value in st.
+template <typename T, int BS>
+__device__ __forceinline__ int stage_blocks(const T* __restrict__ vals, long long nval, int tb, int nb, T* st,
+                                            int lane) {
+  using C = TransferCfg<T, BS>;
+  using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
+  const long long vs = (long long)tb * C::BV;
+  const long long a0 = vs & ~(long long)(C::PER - 1);
+  const int nvec = (int)((vs + (long long)nb * C::BV - a0 + C::PER - 1) / C::PER);
+  for (int q = lane; q < nvec; q += 32) {
+    const long long g = a0 + (long long)q * C::PER;
+    if (g + C::PER <= nval) {
+      *reinterpret_cast<V*>(st + q * C::PER) = __ldcs(reinterpret_cast<const V*>(vals + g));
+    } else {
+#pragma unroll
+      for (int k = 0; k < C::PER; ++k) st[q * C::PER + k] = g + k < nval ? __ldcs(vals + g + k) : T(0);
+    }
+  }
+  return (int)(vs - a0);
+}
+
+// Restriction bc = P^T r, one warp per aggregate, over the aggregate's blocks in
+// the P^T-ordered copy of P: lane k adds blocks k, k + CB, ... of the aggregate
+// in that order, and the six partial sums are combined by a fixed xor tree, so
+// the result is deterministic.
+template <typename T, int BS>
+__global__ void __launch_bounds__(256) sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp,
+                                                          const int* __restrict__ pt_row,
+                                                          const T* __restrict__ ptval, long long nval,
+                                                          const T* __restrict__ r, T* __restrict__ bc) {
+  using C = TransferCfg<T, BS>;
+  __shared__ __align__(16) T sm[8][C::STAGE];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * 8 + wid;
   if (I >= nagg) return;  // whole warps exit together
+  T* st = sm[wid];
   T s[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-  const int t1 = pt_rp[I + 1];
-  for (int t = pt_rp[I] + lane; t < t1; t += 32) {
-    const T* P = ptval + (long long)t * BS * 6;
-    const T* rv = r + (long long)pt_row[t] * BS;
+  const int t0 = pt_rp[I], t1 = pt_rp[I + 1];
+  for (int tb = t0; tb < t1; tb += C::CB) {
+    const int nb = min(C::CB, t1 - tb);
+    // the lane's entries of r are requested before the chunk is staged, so the
+    // two loads' latencies overlap
+    T rv[BS];
+    if (lane < nb) {
+      const T* rr = r + (long long)pt_row[tb + lane] * BS;
 #pragma unroll
-    for (int j = 0; j < BS; ++j) {
-      const T rj = rv[j];
+      for (int j = 0; j < BS; ++j) rv[j] = rr[j];
+    }
+    __syncwarp();  // the previous chunk has been read
+    const int off = stage_blocks<T, BS>(ptval, nval, tb, nb, st, lane);
+    __syncwarp();
+    if (lane < nb) {
+      const T* P = st + off + lane * C::BV;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) s[c] += __ldg(P + j * 6 + c) * rj;
+      for (int j = 0; j < BS; ++j)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) s[c] += P[j * 6 + c] * rv[j];
     }
   }
 #pragma unroll
@@ -780,21 +794,48 @@ __global__ void sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp, cons
     if (lane == c) out = s[c];
   if (lane < 6) bc[(long long)I * 6 + lane] = out;
 }
-// Prolongation x[n*BS+j] += sum_{p in P row n} (P_p xc[col(p)])_j
-template <typename T, int BS>
-__global__ void sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp, const int* __restrict__ p_cl,
-                                  const T* __restrict__ pval, const T* __restrict__ xc, T* __restrict__ x) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nbrow * BS) return;
-  const int n = (int)(i / BS), j = (int)(i % BS);
+
+// Prolongation x += P xc (TWO: x += P (xc + xc2), the two corrections of a
+// W-cycle visit).  A warp owns RW = 32 / BS consecutive fine block rows, lane =
+// row * BS + component; the rows' P blocks and their column ids are contiguous
+// and staged chunk by chunk, and each lane adds its row's blocks in increasing
+// order.
+template <typename T, int BS, bool TWO = false>
+__global__ void __launch_bounds__(256) sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp,
+                                                         const int* __restrict__ p_cl,
+                                                         const T* __restrict__ pval, long long nval,
+                                                         const T* __restrict__ xc, const T* __restrict__ xc2,
+                                                         T* __restrict__ x) {
+  using C = TransferCfg<T, BS>;
+  constexpr int RW = 32 / BS;
+  __shared__ __align__(16) T sm[8][C::STAGE];
+  __shared__ int smc[8][C::CB];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long n0 = ((long long)blockIdx.x * 8 + wid) * RW;
+  if (n0 >= nbrow) return;  // whole warps exit together
+  T* st = sm[wid];
+  int* sc = smc[wid];
+  const int rl = lane / BS, j = lane - rl * BS;
+  const long long n = n0 + rl;
+  const bool act = lane < RW * BS && n < nbrow;
+  const int pa = p_rp[n0], pb = p_rp[min((long long)nbrow, n0 + RW)];
+  const int ps = act ? p_rp[n] : 0, pe = act ? p_rp[n + 1] : 0;
   T s = T(0);
-  for (int p = p_rp[n]; p < p_rp[n + 1]; ++p) {
-    const T* P = pval + (long long)p * BS * 6 + j * 6;
-    const T* xa = xc + (long long)p_cl[p] * 6;
+  for (int cb = pa; cb < pb; cb += C::CB) {
+    const int nb = min(C::CB, pb - cb);
+    __syncwarp();  // the previous chunk has been read
+    for (int q = lane; q < nb; q += 32) sc[q] = __ldcs(p_cl + cb + q);
+    const int off = stage_blocks<T, BS>(pval, nval, cb, nb, st, lane);
+    __syncwarp();
+    const int lo = max(ps, cb), hi = min(pe, cb + nb);
+    for (int p = lo; p < hi; ++p) {
+      const T* P = st + off + (p - cb) * C::BV + j * 6;
+      const long long a = (long long)sc[p - cb] * 6;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) s += __ldcs(P + c) * xa[c];
+      for (int c = 0; c < 6; ++c) s += P[c] * (TWO ? xc[a + c] + xc2[a + c] : xc[a + c]);
+    }
   }
-  x[i] += s;
+  if (act) x[n * BS + j] += s;
 }
 
 template <typename T>
@@ -830,19 +871,34 @@ void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t s
 }
 template <typename T>
 void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st) {
-  const long long n = (long long)v.nagg * 32;  // one warp per aggregate
-  const int blocks = (int)((n + 255) / 256);
+  const int blocks = (v.nagg + 7) / 8;  // one warp per aggregate
+  const long long nval = (long long)v.nnzP * v.A.bs * 6;
   pfem::count_launch();
-  if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
-  else sa_restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
+  if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, nval, r, bc);
+  else sa_restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, nval, r, bc);
+}
+template <typename T>
+static void prolong_launch(const AmgLevel<T>& v, const T* xc, const T* xc2, T* x, cudaStream_t st) {
+  const int rw = 32 / v.A.bs;
+  const long long warps = ((long long)v.A.nbrow + rw - 1) / rw;
+  const int blocks = (int)((warps + 7) / 8);
+  const long long nval = (long long)v.nnzP * v.A.bs * 6;
+  pfem::count_launch();
+  if (v.A.bs == 3) {
+    if (xc2) sa_prolong_kernel<T, 3, true><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc2, x);
+    else sa_prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc, x);
+  } else {
+    if (xc2) sa_prolong_kernel<T, 6, true><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc2, x);
+    else sa_prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc, x);
+  }
 }
 template <typename T>
 void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
-  const long long n = (long long)v.A.nbrow * v.A.bs;
-  const int blocks = (int)((n + 255) / 256);
-  pfem::count_launch();
-  if (v.A.bs == 3) sa_prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, x);
-  else sa_prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, x);
+  prolong_launch<T>(v, xc, nullptr, x, st);
+}
+template <typename T>
+void sa_prolong2(const AmgLevel<T>& v, const T* xc, const T* xc2, T* x, cudaStream_t st) {
+  prolong_launch<T>(v, xc, xc2, x, st);
 }
 
 // ------------------------------------------------------------------ instantiations
@@ -875,7 +931,8 @@ void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st) {
   template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);                            \
   template void sa_setup_level<T>(const AmgLevel<T>&, T, T*, int, cudaStream_t);                   \
   template void sa_restrict<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);                    \
-  template void sa_prolong<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);
+  template void sa_prolong<T>(const AmgLevel<T>&, const T*, T*, cudaStream_t);                     \
+  template void sa_prolong2<T>(const AmgLevel<T>&, const T*, const T*, T*, cudaStream_t);
 PFEM_INST(float)
 PFEM_INST(double)
 template void convert<double, float>(long long, const double*, float*, double, cudaStream_t);

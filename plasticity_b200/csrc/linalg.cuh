@@ -60,6 +60,7 @@ template <typename T> void dense_mv(int n, const T* M, const T* b, T* y, cudaStr
 template <typename T> void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t st);
 template <typename T> void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st);
 template <typename T> void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st);
+template <typename T> void sa_prolong2(const AmgLevel<T>& v, const T* xc, const T* xc2, T* x, cudaStream_t st);
 // Dense inverse of the coarsest operator (dense.cu): its 6 x 6 block pattern
 // (device rp, cl) and values in, the n x n row-major inverse in precision T out;
 // work holds dense_inverse_work_doubles(n) doubles.

@@ -70,7 +70,6 @@ struct BsrMat {
   int* rowptr = nullptr;  // device, nbrow+1
   int* col = nullptr;     // device, nnzb
   VT* val = nullptr;      // device, nnzb*bs*bs (row-major blocks)
-  int maxrow = 0;         // longest block row (0: unknown)
 };
 
 // One level of smoothed-aggregation AMG.  Every fine block row n belongs to
@@ -99,6 +98,8 @@ struct AmgLevel {
   int *c_row = nullptr, *c_cl = nullptr;    // next level's pattern with the row of each block
   // work vectors (length nbrow*bs)
   VT *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
+  // second coarse iteration of a W-cycle visit (levels >= 2): its right-hand side and result
+  VT *b2 = nullptr, *x2 = nullptr;
 };
 
 template <typename VT>
