@@ -37,6 +37,38 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
   T acc[BS];
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
+  if constexpr (BS == 3 && !VEC) {
+    // Two blocks per lane per pass (k and k + 16): both blocks' column ids and
+    // values are requested before either gather of x, so a level-0 row takes one
+    // dependent load chain instead of two; the products are added in the order
+    // k, k + 16, k + 32, ... exactly as one block per pass would add them.
+    for (int k = s + lane; k < e; k += 32) {
+      const int k2 = k + 16;
+      const bool h2 = k2 < e;
+      const int ca = __ldcs(col + k);
+      const int cb = h2 ? __ldcs(col + k2) : 0;
+      const T* Ba = val + (long long)k * 9;
+      const T* Bb = val + (long long)k2 * 9;
+      T ba[9], bb[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) ba[q] = __ldcs(Ba + q);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) bb[q] = h2 ? __ldcs(Bb + q) : T(0);
+      T xa[3], xb[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) xa[j] = x[(long long)ca * 3 + j];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) xb[j] = h2 ? x[(long long)cb * 3 + j] : T(0);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) acc[i] += ba[i * 3 + j] * xa[j];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) acc[i] += bb[i * 3 + j] * xb[j];
+    }
+  } else {
   for (int k = s + lane; k < e; k += 16) {
     const int c = __ldcs(col + k);
     const T* B = val + (long long)k * (BS * BS);
@@ -66,6 +98,7 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
     for (int i = 0; i < BS; ++i)
 #pragma unroll
       for (int j = 0; j < BS; ++j) acc[i] += bv[i * BS + j] * xv[j];
+  }
   }
 #pragma unroll
   for (int i = 0; i < BS; ++i) {
@@ -711,77 +744,33 @@ __global__ void sa_transpose_copy_kernel(int nnzP, const int* __restrict__ pt_bl
   ptval[e] = pval[(long long)pt_blk[t] * (BS * 6) + q];
 }
 
-// Transfer kernels stage the P values they stream in shared memory: a warp copies
-// CB blocks at a time with coalesced 16-byte streaming loads (from the aligned
-// address at or below the chunk's first value; the chunk's values are
-// contiguous), then its lanes take their blocks from shared memory.
-template <typename T, int BS>
-struct TransferCfg {
-  static constexpr int PER = 16 / (int)sizeof(T);
-  static constexpr int BV = BS * 6;  // values of one bs x 6 block
-  static constexpr int CB = BV * (int)sizeof(T) * 32 * 8 <= 40 * 1024 ? 32 : 16;  // blocks per chunk
-  static constexpr int STAGE = CB * BV + PER;
-  static_assert(CB * BV % PER == 0, "chunks end on 16-byte groups");
-};
-
-// Copy blocks [tb, tb + nb) of vals (nval values in all) into st; returns the
-// offset of block tb's first value in st.
-template <typename T, int BS>
-__device__ __forceinline__ int stage_blocks(const T* __restrict__ vals, long long nval, int tb, int nb, T* st,
-                                            int lane) {
-  using C = TransferCfg<T, BS>;
-  using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
-  const long long vs = (long long)tb * C::BV;
-  const long long a0 = vs & ~(long long)(C::PER - 1);
-  const int nvec = (int)((vs + (long long)nb * C::BV - a0 + C::PER - 1) / C::PER);
-  for (int q = lane; q < nvec; q += 32) {
-    const long long g = a0 + (long long)q * C::PER;
-    if (g + C::PER <= nval) {
-      *reinterpret_cast<V*>(st + q * C::PER) = __ldcs(reinterpret_cast<const V*>(vals + g));
-    } else {
-#pragma unroll
-      for (int k = 0; k < C::PER; ++k) st[q * C::PER + k] = g + k < nval ? __ldcs(vals + g + k) : T(0);
-    }
-  }
-  return (int)(vs - a0);
-}
-
-// Restriction bc = P^T r, one warp per aggregate, over the aggregate's blocks in
-// the P^T-ordered copy of P: lane k adds blocks k, k + CB, ... of the aggregate
-// in that order, and the six partial sums are combined by a fixed xor tree, so
-// the result is deterministic.
-template <typename T, int BS>
+// Restriction bc = P^T r, WPA warps per aggregate: the lanes stride over the
+// aggregate's P blocks in the P^T-ordered copy (consecutive lanes read
+// consecutive blocks), each warp combines its six partial sums by a fixed xor
+// tree and the WPA warp sums are added in warp order, so the result is
+// deterministic.  Coarse levels have few aggregates of many blocks each; there
+// WPA = 4 spreads an aggregate over 128 lanes.
+template <typename T, int BS, int WPA>
 __global__ void __launch_bounds__(256) sa_restrict_kernel(int nagg, const int* __restrict__ pt_rp,
                                                           const int* __restrict__ pt_row,
-                                                          const T* __restrict__ ptval, long long nval,
-                                                          const T* __restrict__ r, T* __restrict__ bc) {
-  using C = TransferCfg<T, BS>;
-  __shared__ __align__(16) T sm[8][C::STAGE];
+                                                          const T* __restrict__ ptval, const T* __restrict__ r,
+                                                          T* __restrict__ bc) {
+  __shared__ T part[8][6];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * 8 + wid;
-  if (I >= nagg) return;  // whole warps exit together
-  T* st = sm[wid];
+  const int I = blockIdx.x * (8 / WPA) + wid / WPA;
+  const int w = wid % WPA;
   T s[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-  const int t0 = pt_rp[I], t1 = pt_rp[I + 1];
-  for (int tb = t0; tb < t1; tb += C::CB) {
-    const int nb = min(C::CB, t1 - tb);
-    // the lane's entries of r are requested before the chunk is staged, so the
-    // two loads' latencies overlap
-    T rv[BS];
-    if (lane < nb) {
-      const T* rr = r + (long long)pt_row[tb + lane] * BS;
+  if (I < nagg) {
+    const int t1 = pt_rp[I + 1];
+    for (int t = pt_rp[I] + w * 32 + lane; t < t1; t += 32 * WPA) {
+      const T* P = ptval + (long long)t * BS * 6;
+      const T* rv = r + (long long)pt_row[t] * BS;
 #pragma unroll
-      for (int j = 0; j < BS; ++j) rv[j] = rr[j];
-    }
-    __syncwarp();  // the previous chunk has been read
-    const int off = stage_blocks<T, BS>(ptval, nval, tb, nb, st, lane);
-    __syncwarp();
-    if (lane < nb) {
-      const T* P = st + off + lane * C::BV;
+      for (int j = 0; j < BS; ++j) {
+        const T rj = rv[j];
 #pragma unroll
-      for (int j = 0; j < BS; ++j)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) s[c] += P[j * 6 + c] * rv[j];
+        for (int c = 0; c < 6; ++c) s[c] += __ldg(P + j * 6 + c) * rj;
+      }
     }
   }
 #pragma unroll
@@ -792,50 +781,36 @@ __global__ void __launch_bounds__(256) sa_restrict_kernel(int nagg, const int* _
 #pragma unroll
   for (int c = 1; c < 6; ++c)
     if (lane == c) out = s[c];
-  if (lane < 6) bc[(long long)I * 6 + lane] = out;
-}
-
-// Prolongation x += P xc (TWO: x += P (xc + xc2), the two corrections of a
-// W-cycle visit).  A warp owns RW = 32 / BS consecutive fine block rows, lane =
-// row * BS + component; the rows' P blocks and their column ids are contiguous
-// and staged chunk by chunk, and each lane adds its row's blocks in increasing
-// order.
-template <typename T, int BS, bool TWO = false>
-__global__ void __launch_bounds__(256) sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp,
-                                                         const int* __restrict__ p_cl,
-                                                         const T* __restrict__ pval, long long nval,
-                                                         const T* __restrict__ xc, const T* __restrict__ xc2,
-                                                         T* __restrict__ x) {
-  using C = TransferCfg<T, BS>;
-  constexpr int RW = 32 / BS;
-  __shared__ __align__(16) T sm[8][C::STAGE];
-  __shared__ int smc[8][C::CB];
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long n0 = ((long long)blockIdx.x * 8 + wid) * RW;
-  if (n0 >= nbrow) return;  // whole warps exit together
-  T* st = sm[wid];
-  int* sc = smc[wid];
-  const int rl = lane / BS, j = lane - rl * BS;
-  const long long n = n0 + rl;
-  const bool act = lane < RW * BS && n < nbrow;
-  const int pa = p_rp[n0], pb = p_rp[min((long long)nbrow, n0 + RW)];
-  const int ps = act ? p_rp[n] : 0, pe = act ? p_rp[n + 1] : 0;
-  T s = T(0);
-  for (int cb = pa; cb < pb; cb += C::CB) {
-    const int nb = min(C::CB, pb - cb);
-    __syncwarp();  // the previous chunk has been read
-    for (int q = lane; q < nb; q += 32) sc[q] = __ldcs(p_cl + cb + q);
-    const int off = stage_blocks<T, BS>(pval, nval, cb, nb, st, lane);
-    __syncwarp();
-    const int lo = max(ps, cb), hi = min(pe, cb + nb);
-    for (int p = lo; p < hi; ++p) {
-      const T* P = st + off + (p - cb) * C::BV + j * 6;
-      const long long a = (long long)sc[p - cb] * 6;
+  if constexpr (WPA == 1) {
+    if (I < nagg && lane < 6) bc[(long long)I * 6 + lane] = out;
+  } else {
+    if (lane < 6) part[wid][lane] = out;
+    __syncthreads();
+    if (w == 0 && I < nagg && lane < 6) {
+      T v = part[wid][lane];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) s += P[c] * (TWO ? xc[a + c] + xc2[a + c] : xc[a + c]);
+      for (int q = 1; q < WPA; ++q) v += part[wid + q][lane];
+      bc[(long long)I * 6 + lane] = v;
     }
   }
-  if (act) x[n * BS + j] += s;
+}
+// Prolongation x[n*BS+j] += sum_{p in P row n} (P_p xc[col(p)])_j
+// (TWO: x += P (xc + xc2), the two corrections of a W-cycle visit).
+template <typename T, int BS, bool TWO = false>
+__global__ void sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp, const int* __restrict__ p_cl,
+                                  const T* __restrict__ pval, const T* __restrict__ xc, const T* __restrict__ xc2,
+                                  T* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nbrow * BS) return;
+  const int n = (int)(i / BS), j = (int)(i % BS);
+  T s = T(0);
+  for (int p = p_rp[n]; p < p_rp[n + 1]; ++p) {
+    const T* P = pval + (long long)p * BS * 6 + j * 6;
+    const long long a = (long long)p_cl[p] * 6;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) s += __ldcs(P + c) * (TWO ? xc[a + c] + xc2[a + c] : xc[a + c]);
+  }
+  x[i] += s;
 }
 
 template <typename T>
@@ -869,27 +844,34 @@ void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, int nnzC, cudaStream_t s
                                                                                                v.p_val, v.pt_val);
   }
 }
+// Aggregates below this count get four warps each in the restriction.
+constexpr int kRestrictWideBelow = 4096;
+
 template <typename T>
 void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st) {
-  const int blocks = (v.nagg + 7) / 8;  // one warp per aggregate
-  const long long nval = (long long)v.nnzP * v.A.bs * 6;
+  const bool wide = v.nagg < kRestrictWideBelow;
+  const long long warps = (long long)v.nagg * (wide ? 4 : 1);
+  const int blocks = (int)((warps + 7) / 8);
   pfem::count_launch();
-  if (v.A.bs == 3) sa_restrict_kernel<T, 3><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, nval, r, bc);
-  else sa_restrict_kernel<T, 6><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, nval, r, bc);
+  if (v.A.bs == 3) {
+    if (wide) sa_restrict_kernel<T, 3, 4><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
+    else sa_restrict_kernel<T, 3, 1><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
+  } else {
+    if (wide) sa_restrict_kernel<T, 6, 4><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
+    else sa_restrict_kernel<T, 6, 1><<<blocks, 256, 0, st>>>(v.nagg, v.pt_rp, v.pt_row, v.pt_val, r, bc);
+  }
 }
 template <typename T>
 static void prolong_launch(const AmgLevel<T>& v, const T* xc, const T* xc2, T* x, cudaStream_t st) {
-  const int rw = 32 / v.A.bs;
-  const long long warps = ((long long)v.A.nbrow + rw - 1) / rw;
-  const int blocks = (int)((warps + 7) / 8);
-  const long long nval = (long long)v.nnzP * v.A.bs * 6;
+  const long long n = (long long)v.A.nbrow * v.A.bs;
+  const int blocks = (int)((n + 255) / 256);
   pfem::count_launch();
   if (v.A.bs == 3) {
-    if (xc2) sa_prolong_kernel<T, 3, true><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc2, x);
-    else sa_prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc, x);
+    if (xc2) sa_prolong_kernel<T, 3, true><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, xc2, x);
+    else sa_prolong_kernel<T, 3><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, xc, x);
   } else {
-    if (xc2) sa_prolong_kernel<T, 6, true><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc2, x);
-    else sa_prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, nval, xc, xc, x);
+    if (xc2) sa_prolong_kernel<T, 6, true><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, xc2, x);
+    else sa_prolong_kernel<T, 6><<<blocks, 256, 0, st>>>(v.A.nbrow, v.p_rp, v.p_cl, v.p_val, xc, xc, x);
   }
 }
 template <typename T>
