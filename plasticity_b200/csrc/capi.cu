@@ -117,6 +117,7 @@ struct pfem_ctx {
   uint8_t* dNloc = nullptr;
   int max_row = 0;
   bool colored_assembly = false;
+  bool coarse_tail = true;  // the cycle's bottom in one cluster launch where it applies
   float* dKbuf32 = nullptr;
   double* dKbuf64 = nullptr;
   double* dFbuf = nullptr;
@@ -182,11 +183,23 @@ cudaError_t dalloc(pfem_ctx* ctx, T** p, size_t n) {
   if (e == cudaSuccess) ctx->allocs.push_back((void*)*p);
   return e;
 }
+// Host transfers of the API run on the library's stream, which is non-blocking:
+// a legacy-stream cudaMemcpy is not ordered with its kernels (a pageable
+// host-to-device copy may still be in flight when it returns, and a
+// device-to-host copy does not wait for kernels queued on the stream).
+cudaError_t h2d(const pfem_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->st);
+  return e == cudaSuccess ? cudaStreamSynchronize(ctx->st) : e;
+}
+cudaError_t d2h(const pfem_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->st);
+  return e == cudaSuccess ? cudaStreamSynchronize(ctx->st) : e;
+}
 template <typename T>
 cudaError_t upload(pfem_ctx* ctx, T** p, const std::vector<T>& h) {
   cudaError_t e = dalloc(ctx, p, h.size());
   if (e != cudaSuccess) return e;
-  if (!h.empty()) e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+  if (!h.empty()) e = h2d(ctx, *p, h.data(), h.size() * sizeof(T));
   return e;
 }
 
@@ -831,6 +844,19 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
 // Chebyshev smoothing (block-Jacobi preconditioned) on level l:
 // x <- x + p(D^-1 A) D^-1 (b - A x), degree A.cheb_degree, interval
 // [lmax/30, lmax].  zero: x enters as 0.
+// Degree-2 coefficients on [lmax/30, lmax]: x2 = x0 + d0 + d1 with d0 = r0 / th,
+// r0 = Dinv (b - A x0), r1 = r0 - Dinv A d0, d1 = c1 r1 + (c2 - 1) d0.
+template <typename T>
+void cheb2_coeffs(const AmgLevel<T>& v, T* inv_th, T* c1, T* c2) {
+  const double lmx = (double)v.lmax, lmn = lmx / 30.0;
+  const double th = 0.5 * (lmx + lmn), de = 0.5 * (lmx - lmn);
+  const double sg = th / de, rho = 1.0 / sg;
+  const double rn = 1.0 / (2.0 * sg - rho);
+  *inv_th = T(1.0 / th);
+  *c1 = T(2.0 * rn / de);
+  *c2 = T(1.0 + rn * rho);
+}
+
 template <typename T>
 void cheb(pfem_ctx* ctx, AmgLevel<T>& v, int degree, const T* b, T* x, bool zero) {
   const long long n = (long long)v.A.nbrow * v.A.bs;
@@ -839,13 +865,11 @@ void cheb(pfem_ctx* ctx, AmgLevel<T>& v, int degree, const T* b, T* x, bool zero
   const double sg = th / de;
   double rho = 1.0 / sg;
   if (degree == 2) {
-    // x2 = x0 + d0 + d1 with d0 = r0 / th, r0 = Dinv (b - A x0), r1 = r0 - Dinv A d0,
-    // d1 = (2 rn / de) r1 + rn rho d0: one block-Jacobi pass (or a fused
-    // residual pass) and one fused SpMV pass.
-    const double rn = 1.0 / (2.0 * sg - rho);
-    const T c1 = T(2.0 * rn / de), c2 = T(1.0 + rn * rho);
-    if (zero) blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, b, v.r, T(1.0 / th), v.d, ctx->st);
-    else bsr_residual_precond<T>(v.A, v.dinv, x, b, v.r, v.d, T(1.0 / th), ctx->st);
+    // one block-Jacobi pass (or a fused residual pass) and one fused SpMV pass
+    T inv_th, c1, c2;
+    cheb2_coeffs<T>(v, &inv_th, &c1, &c2);
+    if (zero) blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, b, v.r, inv_th, v.d, ctx->st);
+    else bsr_residual_precond<T>(v.A, v.dinv, x, b, v.r, v.d, inv_th, ctx->st);
     bsr_cheb2<T>(v.A, v.dinv, v.d, v.r, x, zero, c1, c2, ctx->st);
     return;
   }
@@ -878,6 +902,19 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
   T* bn = (l + 1 < L) ? A.lv[l + 1].b : A.cb;
   T* xn = (l + 1 < L) ? A.lv[l + 1].x : A.cx;
   sa_restrict<T>(v, v.t, bn, ctx->st);
+  if (l + 1 == L - 1 && ctx->coarse_tail && A.cheb_degree == 2 && A.lv[l + 1].A.bs == 6 &&
+      A.lv[l + 1].A.nbrow <= kCoarseTailMaxRows) {
+    // the last non-dense level (once, or twice below level 0) and the dense
+    // solve in one launch
+    AmgLevel<T>& c = A.lv[l + 1];
+    T inv_th, c1, c2;
+    cheb2_coeffs<T>(c, &inv_th, &c1, &c2);
+    coarse_tail<T>(c, A.coarse_n, A.coarse_inv, A.cb, A.cx, bn, xn, l >= 1, inv_th, c1, c2, ctx->st);
+    if (l >= 1) sa_prolong2<T>(v, xn, c.x2, x, ctx->st);
+    else sa_prolong<T>(v, xn, x, ctx->st);
+    cheb<T>(ctx, v, A.cheb_degree, b, x, false);
+    return;
+  }
   if (l + 1 < L) vcycle<T>(ctx, l + 1, bn, xn);
   else dense_mv<T>(A.coarse_n, A.coarse_inv, bn, xn, ctx->st);
   if (l >= 1 && l + 1 < L) {
@@ -1526,7 +1563,7 @@ static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t*
     if (dims) { dims[0] = n; dims[1] = n; }
     if (!out) return PFEM_OK;
     std::vector<T> v((size_t)n * n);
-    CK(cudaMemcpy(v.data(), A.coarse_inv, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, v.data(), A.coarse_inv, v.size() * sizeof(T)));
     for (size_t i = 0; i < v.size(); ++i) out[i] = (double)v[i];
     return PFEM_OK;
   }
@@ -1539,7 +1576,7 @@ static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t*
     const long long nb = hrp[h.nbrow];
     std::vector<T> v((size_t)nb * bs * bs);
     const T* src = level < L ? A.lv[level].A.val : A.coarse_val;
-    CK(cudaMemcpy(v.data(), src, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, v.data(), src, v.size() * sizeof(T)));
     std::fill(out, out + (size_t)nr * nr, 0.0);
     for (int I = 0; I < h.nbrow; ++I)
       for (int k = hrp[I]; k < hrp[I + 1]; ++k)
@@ -1551,7 +1588,7 @@ static int amg_dense_t(pfem_ctx* ctx, int level, int what, double* out, int64_t*
     if (dims) { dims[0] = nr; dims[1] = nc; }
     if (!out) return PFEM_OK;
     std::vector<T> v((size_t)h.p_cl.size() * bs * 6);
-    CK(cudaMemcpy(v.data(), A.lv[level].p_val, v.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, v.data(), A.lv[level].p_val, v.size() * sizeof(T)));
     std::fill(out, out + (size_t)nr * nc, 0.0);
     for (int n = 0; n < h.nbrow; ++n)
       for (int p = h.p_rp[n]; p < h.p_rp[n + 1]; ++p)
@@ -1843,6 +1880,8 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     for (int64_t n = 0; n < nn; ++n) ctx->max_row = std::max(ctx->max_row, ctx->browptr[n + 1] - ctx->browptr[n]);
     const char* am = getenv("PFEM_ASSEMBLY");
     ctx->colored_assembly = am && std::string(am) == "colored";
+    const char* ct = getenv("PFEM_COARSE_TAIL");
+    ctx->coarse_tail = !(ct && std::string(ct) == "0");
   }
   if (sigy0_e) {
     std::vector<double> s(sigy0_e, sigy0_e + ne);
@@ -1898,7 +1937,7 @@ int pfem_inversion_info(const pfem_ctx* ctx, int64_t* e, int32_t* g, double* J) 
   if (!ctx) return PFEM_ERR_BAD_ARG;
   if (ctx->device < 0) return PFEM_ERR_STATE;
   DevStatus s;
-  if (cudaMemcpy(&s, ctx->dStatus, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (d2h(ctx, &s, ctx->dStatus, sizeof(s)) != cudaSuccess) return PFEM_ERR_CUDA;
   if (e) *e = s.code ? s.e : 0;
   if (g) *g = s.code ? s.g : 0;
   if (J) *J = s.code ? s.J : 0.0;
@@ -1979,9 +2018,9 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
     // without boundary conditions rather than with a half-updated set
     ctx->bcs_set = false;
     CK(cudaStreamSynchronize(ctx->st));
-    CK(cudaMemcpy(b.vals, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b.ramp, ramp.data(), ramp.size() * sizeof(uint8_t), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b.fn, fn.data(), fn.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, b.vals, vals.data(), vals.size() * sizeof(double)));
+    CK(h2d(ctx, b.ramp, ramp.data(), ramp.size() * sizeof(uint8_t)));
+    CK(h2d(ctx, b.fn, fn.data(), fn.size() * sizeof(double)));
     ctx->bcs_set = true;
     return PFEM_OK;
   }
@@ -2083,13 +2122,13 @@ int pfem_set_state(pfem_ctx* ctx, const double* cpi, const double* alpha, const 
     std::vector<double> t(6 * ngp);
     for (long long g = 0; g < ngp; ++g)
       for (int k = 0; k < 6; ++k) t[k * ngp + g] = h[g * 6 + k];
-    CK(cudaMemcpy(d, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, d, t.data(), t.size() * sizeof(double)));
     return PFEM_OK;
   };
   int rc;
   if (cpi && (rc = put(cpi, ctx->dCpi))) return rc;
   if (epsp && (rc = put(epsp, ctx->dEpsp))) return rc;
-  if (alpha) CK(cudaMemcpy(ctx->dAlpha, alpha, ngp * sizeof(double), cudaMemcpyHostToDevice));
+  if (alpha) CK(h2d(ctx, ctx->dAlpha, alpha, ngp * sizeof(double)));
   return PFEM_OK;
 }
 
@@ -2104,7 +2143,7 @@ int pfem_get_back_stress(const pfem_ctx* ctx, double* beta) {
   cudaSetDevice(ctx->device);
   if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return PFEM_ERR_CUDA;
   std::vector<double> t(6 * ngp);
-  if (cudaMemcpy(t.data(), ctx->dBeta, t.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (d2h(ctx, t.data(), ctx->dBeta, t.size() * sizeof(double)) != cudaSuccess)
     return PFEM_ERR_CUDA;
   for (long long g = 0; g < ngp; ++g)
     for (int k = 0; k < 6; ++k) beta[g * 6 + k] = t[k * ngp + g];
@@ -2121,7 +2160,7 @@ int pfem_set_back_stress(pfem_ctx* ctx, const double* beta) {
   for (long long g = 0; g < ngp; ++g)
     for (int k = 0; k < 6; ++k) t[k * ngp + g] = beta[g * 6 + k];
   CK(cudaStreamSynchronize(ctx->st));
-  CK(cudaMemcpy(ctx->dBeta, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(h2d(ctx, ctx->dBeta, t.data(), t.size() * sizeof(double)));
   return PFEM_OK;
 }
 
@@ -2154,15 +2193,15 @@ int pfem_assemble(pfem_ctx* ctx, const double* U, int32_t commit, int32_t precis
     if (rc) return rc;
     ctx->tangent_prec = -1;  // not imposed
   }
-  if (R && !commit) CK(cudaMemcpy(R, ctx->dR, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  if (R && !commit) CK(d2h(ctx, R, ctx->dR, ctx->ndof * sizeof(double)));
   if (Kvals && !commit) {
     const size_t nv = (size_t)ctx->nnzb * 9;
     std::vector<double> kv(nv);
     if (prec == PFEM_FP64) {
-      CK(cudaMemcpy(kv.data(), ctx->dK64, nv * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(d2h(ctx, kv.data(), ctx->dK64, nv * sizeof(double)));
     } else {
       std::vector<float> kf(nv);
-      CK(cudaMemcpy(kf.data(), ctx->dK32, nv * sizeof(float), cudaMemcpyDeviceToHost));
+      CK(d2h(ctx, kf.data(), ctx->dK32, nv * sizeof(float)));
       for (size_t i = 0; i < nv; ++i) kv[i] = kf[i];
     }
     // block (n, m) entry (i, k) -> CSR row 3n+i, position 3*t + k in that row
@@ -2200,7 +2239,7 @@ static int mlp_alloc(pfem_ctx* ctx) {
 
 static int mlp_check_err(pfem_ctx* ctx) {
   int e = 0;
-  CK(cudaMemcpy(&e, ctx->mlp.err, sizeof(int), cudaMemcpyDeviceToHost));
+  CK(d2h(ctx, &e, ctx->mlp.err, sizeof(int)));
   if (e) {
     cudaMemset(ctx->mlp.err, 0, sizeof(int));
     return fail(ctx, PFEM_ERR_CUDA, "tensor-core MMA wait timed out in the predictor kernel");
@@ -2342,7 +2381,7 @@ int pfem_predict(pfem_ctx* ctx, double lambda, const pfem_solve_opts* o, double*
     rc = residual_system(ctx, o->precision, lambda, r_extrap, &tm.asm_ms);
     if (rc) return rc;
   }
-  if (U) CK(cudaMemcpy(U, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  if (U) CK(d2h(ctx, U, ctx->dU, ctx->ndof * sizeof(double)));
   return PFEM_OK;
 }
 
@@ -2423,7 +2462,7 @@ int pfem_residual(pfem_ctx* ctx, double lambda, int32_t precision, double* rnorm
   int rc = residual_system(ctx, precision == PFEM_MIXED ? PFEM_MIXED : PFEM_FP64, lambda, &rn, &t);
   if (rc) return rc;
   if (rnorm) *rnorm = rn;
-  if (R) CK(cudaMemcpy(R, ctx->dR, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+  if (R) CK(d2h(ctx, R, ctx->dR, ctx->ndof * sizeof(double)));
   return PFEM_OK;
 }
 
@@ -2441,19 +2480,19 @@ int pfem_linear_solve(pfem_ctx* ctx, const double* b, double* x, double rtol, in
   if (prec == PFEM_FP64) {
     if (rebuild_pc || !ctx->amg64.built) { rc = amg_setup<double>(ctx, o->cheb_degree); if (rc) return rc; }
     ctx->amg64.lv[0].A.val = ctx->dK64;
-    CK(cudaMemcpy(ctx->kw64.b, hb.data(), ctx->ndof * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, ctx->kw64.b, hb.data(), ctx->ndof * sizeof(double)));
     rc = krylov<double>(ctx, o->krylov, rtol, o->krylov_itmax, &it, &conv);
     if (rc) return rc;
-    CK(cudaMemcpy(x, ctx->kw64.x, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, x, ctx->kw64.x, ctx->ndof * sizeof(double)));
   } else {
     if (rebuild_pc || !ctx->amg32.built) { rc = amg_setup<float>(ctx, o->cheb_degree); if (rc) return rc; }
     ctx->amg32.lv[0].A.val = ctx->dK32;
     std::vector<float> hf(hb.begin(), hb.end());
-    CK(cudaMemcpy(ctx->kw32.b, hf.data(), ctx->ndof * sizeof(float), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, ctx->kw32.b, hf.data(), ctx->ndof * sizeof(float)));
     rc = krylov<float>(ctx, o->krylov, rtol, o->krylov_itmax, &it, &conv);
     if (rc) return rc;
     std::vector<float> xf(ctx->ndof);
-    CK(cudaMemcpy(xf.data(), ctx->kw32.x, ctx->ndof * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, xf.data(), ctx->kw32.x, ctx->ndof * sizeof(float)));
     for (long long i = 0; i < ctx->ndof; ++i) x[i] = xf[i];
   }
   if (niter) *niter = it;
@@ -2466,16 +2505,16 @@ int pfem_amg_apply(pfem_ctx* ctx, const double* r, double* z) {
   cudaSetDevice(ctx->device);
   const long long n = ctx->ndof;
   if (ctx->tangent_prec == PFEM_FP64 && ctx->amg64.built) {
-    CK(cudaMemcpy(ctx->kw64.r, r, n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, ctx->kw64.r, r, n * sizeof(double)));
     vcycle<double>(ctx, 0, ctx->kw64.r, ctx->kw64.z);
     CKL();
-    CK(cudaMemcpy(z, ctx->kw64.z, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, z, ctx->kw64.z, n * sizeof(double)));
   } else if (ctx->tangent_prec == PFEM_MIXED && ctx->amg32.built) {
     std::vector<float> f(r, r + n);
-    CK(cudaMemcpy(ctx->kw32.r, f.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, ctx->kw32.r, f.data(), n * sizeof(float)));
     vcycle<float>(ctx, 0, ctx->kw32.r, ctx->kw32.z);
     CKL();
-    CK(cudaMemcpy(f.data(), ctx->kw32.z, n * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, f.data(), ctx->kw32.z, n * sizeof(float)));
     for (long long i = 0; i < n; ++i) z[i] = f[i];
   } else {
     return fail(ctx, PFEM_ERR_STATE, "no AMG hierarchy built for the resident tangent");
@@ -2566,9 +2605,9 @@ int pfem_get_state(const pfem_ctx* ctx, double* U, double* tau, double* alpha, d
   cudaSetDevice(ctx->device);
   if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return PFEM_ERR_CUDA;
   const long long ngp = ctx->ngp;
-  if (U && cudaMemcpy(U, ctx->dU, ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
-  if (alpha && cudaMemcpy(alpha, ctx->dAlpha, ngp * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
-  if (flags && cudaMemcpy(flags, ctx->dFlags, ngp, cudaMemcpyDeviceToHost) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (U && d2h(ctx, U, ctx->dU, ctx->ndof * sizeof(double)) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (alpha && d2h(ctx, alpha, ctx->dAlpha, ngp * sizeof(double)) != cudaSuccess) return PFEM_ERR_CUDA;
+  if (flags && d2h(ctx, flags, ctx->dFlags, ngp) != cudaSuccess) return PFEM_ERR_CUDA;
   if (tau && download_aos(c, ctx->dTau, tau)) return PFEM_ERR_CUDA;
   if (cpi && download_aos(c, ctx->dCpi, cpi)) return PFEM_ERR_CUDA;
   if (epsp && download_aos(c, ctx->dEpsp, epsp)) return PFEM_ERR_CUDA;
@@ -2676,7 +2715,7 @@ int pfem_mlp_init(pfem_ctx* ctx, uint64_t seed) {
   const int oW3 = oW2 + H * H + H;
   for (int o = 0; o < 3; ++o)
     for (int h = 0; h < H; ++h) p[oW3 + o * H + h] = (float)(uni() * std::sqrt(6.0 / H) * 0.1);
-  CK(cudaMemcpy(ctx->mlp.w, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CK(h2d(ctx, ctx->mlp.w, p.data(), p.size() * sizeof(float)));
   CK(cudaMemset(ctx->mlp.m, 0, MLP_NPARAMS * sizeof(float)));
   CK(cudaMemset(ctx->mlp.v, 0, MLP_NPARAMS * sizeof(float)));
   ctx->mlp.adam_t = 0;
@@ -2691,9 +2730,9 @@ int pfem_mlp_params(pfem_ctx* ctx, int32_t op, float* p, int64_t n) {
   int rc = mlp_alloc(ctx);
   if (rc) return rc;
   if (op == 0) {
-    CK(cudaMemcpy(p, ctx->mlp.w, MLP_NPARAMS * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, p, ctx->mlp.w, MLP_NPARAMS * sizeof(float)));
   } else {
-    CK(cudaMemcpy(ctx->mlp.w, p, MLP_NPARAMS * sizeof(float), cudaMemcpyHostToDevice));
+    CK(h2d(ctx, ctx->mlp.w, p, MLP_NPARAMS * sizeof(float)));
     ctx->mlp.ready = true;
   }
   return PFEM_OK;
@@ -2711,11 +2750,11 @@ int pfem_mlp_forward(pfem_ctx* ctx, const float* feats, int64_t n, float* out) {
   CK(tmp.alloc(&df, (size_t)n * MLP_NFEAT * sizeof(float)));
   CK(tmp.alloc(&db, (size_t)n * 32));
   CK(tmp.alloc(&dy, (size_t)n * 3 * sizeof(float)));
-  CK(cudaMemcpy(df, feats, (size_t)n * MLP_NFEAT * sizeof(float), cudaMemcpyHostToDevice));
+  CK(h2d(ctx, df, feats, (size_t)n * MLP_NFEAT * sizeof(float)));
   mlp_pack_features(df, n, db, ctx->st);
   rc = mlp_launch(false, ctx->mlp.w, db, nullptr, nullptr, n, dy, nullptr, nullptr, ctx->mlp.err, 148, ctx->st);
   CK(cudaStreamSynchronize(ctx->st));
-  CK(cudaMemcpy(out, dy, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+  CK(d2h(ctx, out, dy, (size_t)n * 3 * sizeof(float)));
   if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
   return mlp_check_err(ctx);
 }
@@ -2732,17 +2771,17 @@ int pfem_mlp_loss_grad(pfem_ctx* ctx, const float* feats, const float* targets, 
   CK(tmp.alloc(&df, (size_t)n * MLP_NFEAT * sizeof(float)));
   CK(tmp.alloc(&db, (size_t)n * 32));
   CK(tmp.alloc(&dt, (size_t)n * 3 * sizeof(float)));
-  CK(cudaMemcpy(df, feats, (size_t)n * MLP_NFEAT * sizeof(float), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dt, targets, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice));
+  CK(h2d(ctx, df, feats, (size_t)n * MLP_NFEAT * sizeof(float)));
+  CK(h2d(ctx, dt, targets, (size_t)n * 3 * sizeof(float)));
   mlp_pack_features(df, n, db, ctx->st);
   CK(cudaMemsetAsync(ctx->mlp.g, 0, MLP_NPARAMS * sizeof(float), ctx->st));
   CK(cudaMemsetAsync(ctx->mlp.loss, 0, sizeof(float), ctx->st));
   rc = mlp_launch(true, ctx->mlp.w, db, dt, nullptr, n, nullptr, ctx->mlp.g, ctx->mlp.loss, ctx->mlp.err, 148,
                   ctx->st);
   CK(cudaStreamSynchronize(ctx->st));
-  if (grad) CK(cudaMemcpy(grad, ctx->mlp.g, MLP_NPARAMS * sizeof(float), cudaMemcpyDeviceToHost));
+  if (grad) CK(d2h(ctx, grad, ctx->mlp.g, MLP_NPARAMS * sizeof(float)));
   float l = 0;
-  CK(cudaMemcpy(&l, ctx->mlp.loss, sizeof(float), cudaMemcpyDeviceToHost));
+  CK(d2h(ctx, &l, ctx->mlp.loss, sizeof(float)));
   if (loss) *loss = l / (3.0f * (float)n);
   if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor kernel launch failed");
   return mlp_check_err(ctx);
@@ -2799,7 +2838,7 @@ int pfem_mlp_train(pfem_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64
   CK(cudaStreamSynchronize(ctx->st));
   if (losses) {
     std::vector<float> h(steps);
-    CK(cudaMemcpy(h.data(), dl, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(d2h(ctx, h.data(), dl, (size_t)steps * sizeof(float)));
     for (int k = 0; k < steps; ++k) losses[k] = h[k] / (3.0f * (float)batch);
   }
   if (rc) return fail(ctx, PFEM_ERR_CUDA, "predictor training kernel launch failed");

@@ -37,38 +37,6 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
   T acc[BS];
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
-  if constexpr (BS == 3 && !VEC) {
-    // Two blocks per lane per pass (k and k + 16): both blocks' column ids and
-    // values are requested before either gather of x, so a level-0 row takes one
-    // dependent load chain instead of two; the products are added in the order
-    // k, k + 16, k + 32, ... exactly as one block per pass would add them.
-    for (int k = s + lane; k < e; k += 32) {
-      const int k2 = k + 16;
-      const bool h2 = k2 < e;
-      const int ca = __ldcs(col + k);
-      const int cb = h2 ? __ldcs(col + k2) : 0;
-      const T* Ba = val + (long long)k * 9;
-      const T* Bb = val + (long long)k2 * 9;
-      T ba[9], bb[9];
-#pragma unroll
-      for (int q = 0; q < 9; ++q) ba[q] = __ldcs(Ba + q);
-#pragma unroll
-      for (int q = 0; q < 9; ++q) bb[q] = h2 ? __ldcs(Bb + q) : T(0);
-      T xa[3], xb[3];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) xa[j] = x[(long long)ca * 3 + j];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) xb[j] = h2 ? x[(long long)cb * 3 + j] : T(0);
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) acc[i] += ba[i * 3 + j] * xa[j];
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) acc[i] += bb[i * 3 + j] * xb[j];
-    }
-  } else {
   for (int k = s + lane; k < e; k += 16) {
     const int c = __ldcs(col + k);
     const T* B = val + (long long)k * (BS * BS);
@@ -98,7 +66,6 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
     for (int i = 0; i < BS; ++i)
 #pragma unroll
       for (int j = 0; j < BS; ++j) acc[i] += bv[i * BS + j] * xv[j];
-  }
   }
 #pragma unroll
   for (int i = 0; i < BS; ++i) {
