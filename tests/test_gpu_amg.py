@@ -75,7 +75,7 @@ def test_coarse_tail_matches_phase_kernels(n, precision, monkeypatch):
     for tail in ("1", "0"):
         monkeypatch.setenv("PFEM_COARSE_TAIL", tail)
         M, R = _model(n, precision)
-        M.linear_solve(-R, rtol=1e-6, rebuild=True, precision=precision)
+        M.linear_solve(-R, rtol=1e-4, rebuild=True, precision=precision)  # builds the hierarchy
         k0 = L.lib().pfem_kernel_launches()
         z.append(M.amg_apply(R))
         launches.append(L.lib().pfem_kernel_launches() - k0)
