@@ -711,6 +711,21 @@ __global__ void sa_transpose_copy_kernel(int nnzP, const int* __restrict__ pt_bl
   ptval[e] = pval[(long long)pt_blk[t] * (BS * 6) + q];
 }
 
+// Six consecutive values from an address that is 8-byte aligned (float) or
+// 16-byte aligned (double), as three 8- or 16-byte loads: every 6-value row of a
+// bs x 6 transfer block and every 6-vector of a coarse level is.
+template <typename T, bool STREAM>
+__device__ __forceinline__ void load6(const T* __restrict__ p, T* v) {
+  using V2 = typename std::conditional<std::is_same<T, float>::value, float2, double2>::type;
+  const V2* q = reinterpret_cast<const V2*>(p);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const V2 w = STREAM ? __ldcs(q + k) : __ldg(q + k);
+    v[2 * k] = w.x;
+    v[2 * k + 1] = w.y;
+  }
+}
+
 // Restriction bc = P^T r, WPA warps per aggregate: the lanes stride over the
 // aggregate's P blocks in the P^T-ordered copy (consecutive lanes read
 // consecutive blocks), each warp combines its six partial sums by a fixed xor
@@ -735,8 +750,10 @@ __global__ void __launch_bounds__(256) sa_restrict_kernel(int nagg, const int* _
 #pragma unroll
       for (int j = 0; j < BS; ++j) {
         const T rj = rv[j];
+        T pv[6];
+        load6<T, false>(P + j * 6, pv);
 #pragma unroll
-        for (int c = 0; c < 6; ++c) s[c] += __ldg(P + j * 6 + c) * rj;
+        for (int c = 0; c < 6; ++c) s[c] += pv[c] * rj;
       }
     }
   }
@@ -774,8 +791,17 @@ __global__ void sa_prolong_kernel(int nbrow, const int* __restrict__ p_rp, const
   for (int p = p_rp[n]; p < p_rp[n + 1]; ++p) {
     const T* P = pval + (long long)p * BS * 6 + j * 6;
     const long long a = (long long)p_cl[p] * 6;
+    T pv[6], xv[6];
+    load6<T, true>(P, pv);
+    load6<T, false>(xc + a, xv);
+    if (TWO) {
+      T x2v[6];
+      load6<T, false>(xc2 + a, x2v);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) s += __ldcs(P + c) * (TWO ? xc[a + c] + xc2[a + c] : xc[a + c]);
+      for (int c = 0; c < 6; ++c) xv[c] += x2v[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) s += pv[c] * xv[c];
   }
   x[i] += s;
 }

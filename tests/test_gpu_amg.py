@@ -69,7 +69,9 @@ def test_coarse_tail_matches_phase_kernels(n, precision, monkeypatch):
     per phase.  24^3: one visit to level 1 (the last non-dense level, about 580 block
     rows); 64^3: two visits to level 2 (512 block rows) below the level-1 W.  The
     cluster sums the restriction over 32 warps instead of 4, so the results agree
-    to rounding; the launch count shows which path ran."""
+    to rounding: 1e-12 in FP64; in FP32 the coarse solve amplifies the reordered
+    sums' rounding (2e-5 relative measured at 24^3), hence 1e-4.  The launch count
+    shows which path ran."""
     from plasticity_b200 import _lib as L
     z, launches = [], []
     for tail in ("1", "0"):
@@ -80,7 +82,7 @@ def test_coarse_tail_matches_phase_kernels(n, precision, monkeypatch):
         z.append(M.amg_apply(R))
         launches.append(L.lib().pfem_kernel_launches() - k0)
     assert launches[0] < launches[1], launches
-    tol = 1e-12 if precision == "fp64" else 1e-5
+    tol = 1e-12 if precision == "fp64" else 1e-4
     assert np.linalg.norm(z[0] - z[1]) <= tol * np.linalg.norm(z[1])
 
 
