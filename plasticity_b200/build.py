@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpfem_b200.so")
-SOURCES = ["capi.cu", "coarse.cu", "dense.cu", "element.cu", "linalg.cu", "mlp.cu", "noalloc.cu", "topology.cu"]
+SOURCES = ["capi.cu", "dense.cu", "element.cu", "linalg.cu", "mlp.cu", "noalloc.cu", "topology.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O3,-march=x86-64-v3", "-shared", "-cudart", "static"]

@@ -117,7 +117,6 @@ struct pfem_ctx {
   uint8_t* dNloc = nullptr;
   int max_row = 0;
   bool colored_assembly = false;
-  bool coarse_tail = true;  // the cycle's bottom in one cluster launch where it applies
   float* dKbuf32 = nullptr;
   double* dKbuf64 = nullptr;
   double* dFbuf = nullptr;
@@ -902,19 +901,6 @@ void vcycle(pfem_ctx* ctx, int l, const T* b, T* x) {
   T* bn = (l + 1 < L) ? A.lv[l + 1].b : A.cb;
   T* xn = (l + 1 < L) ? A.lv[l + 1].x : A.cx;
   sa_restrict<T>(v, v.t, bn, ctx->st);
-  if (l + 1 == L - 1 && ctx->coarse_tail && A.cheb_degree == 2 && A.lv[l + 1].A.bs == 6 &&
-      A.lv[l + 1].A.nbrow <= kCoarseTailMaxRows) {
-    // the last non-dense level (once, or twice below level 0) and the dense
-    // solve in one launch
-    AmgLevel<T>& c = A.lv[l + 1];
-    T inv_th, c1, c2;
-    cheb2_coeffs<T>(c, &inv_th, &c1, &c2);
-    coarse_tail<T>(c, A.coarse_n, A.coarse_inv, A.cb, A.cx, bn, xn, l >= 1, inv_th, c1, c2, ctx->st);
-    if (l >= 1) sa_prolong2<T>(v, xn, c.x2, x, ctx->st);
-    else sa_prolong<T>(v, xn, x, ctx->st);
-    cheb<T>(ctx, v, A.cheb_degree, b, x, false);
-    return;
-  }
   if (l + 1 < L) vcycle<T>(ctx, l + 1, bn, xn);
   else dense_mv<T>(A.coarse_n, A.coarse_inv, bn, xn, ctx->st);
   if (l >= 1 && l + 1 < L) {
@@ -1880,8 +1866,6 @@ int pfem_create(pfem_ctx** out, const double* nodes, int64_t nn, const int64_t* 
     for (int64_t n = 0; n < nn; ++n) ctx->max_row = std::max(ctx->max_row, ctx->browptr[n + 1] - ctx->browptr[n]);
     const char* am = getenv("PFEM_ASSEMBLY");
     ctx->colored_assembly = am && std::string(am) == "colored";
-    const char* ct = getenv("PFEM_COARSE_TAIL");
-    ctx->coarse_tail = !(ct && std::string(ct) == "0");
   }
   if (sigy0_e) {
     std::vector<double> s(sigy0_e, sigy0_e + ne);

@@ -61,14 +61,6 @@ template <typename T> void sa_setup_level(const AmgLevel<T>& v, T w, T* cval, in
 template <typename T> void sa_restrict(const AmgLevel<T>& v, const T* r, T* bc, cudaStream_t st);
 template <typename T> void sa_prolong(const AmgLevel<T>& v, const T* xc, T* x, cudaStream_t st);
 template <typename T> void sa_prolong2(const AmgLevel<T>& v, const T* xc, const T* xc2, T* x, cudaStream_t st);
-// The last non-dense level and the dense solve in one thread-block cluster
-// launch (coarse.cu): one V visit with right-hand side b into x (zero start) and,
-// with twice, a second from the level's residual into v.x2 (a W-cycle's two
-// coarse iterations).  For levels of 6 x 6 blocks and at most kCoarseTailMaxRows
-// block rows, degree-2 Chebyshev smoothing with the given coefficients.
-constexpr int kCoarseTailMaxRows = 1024;
-template <typename T> void coarse_tail(const AmgLevel<T>& v, int nc, const T* cinv, T* cb, T* cx, const T* b, T* x,
-                                       bool twice, T inv_th, T c1, T c2, cudaStream_t st);
 // Dense inverse of the coarsest operator (dense.cu): its 6 x 6 block pattern
 // (device rp, cl) and values in, the n x n row-major inverse in precision T out;
 // work holds dense_inverse_work_doubles(n) doubles.
