@@ -766,6 +766,8 @@ void dense_inverse_host(int n, std::vector<double>& a, std::vector<double>& inv)
 // (the reference's reuse policy, Solver.jl:243-245).
 template <typename T>
 int amg_setup(pfem_ctx* ctx, int cheb_degree) {
+  const bool dbg = getenv("PFEM_DEBUG_AMG") != nullptr;
+  auto ts = std::chrono::steady_clock::now();
   if (!ctx->amg_struct) build_amg_structure(ctx);
   int rc = amg_alloc<T>(ctx);
   if (rc) return rc;
@@ -805,6 +807,8 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     sa_setup_level<T>(v, omega, cval, nnzC, ctx->st);
     CKL();
   }
+  if (dbg) cudaStreamSynchronize(ctx->st);
+  auto tl = std::chrono::steady_clock::now();
   // coarsest operator: dense inverse, on the device (blocked Gauss-Jordan) for
   // large coarsest levels, on the host with partial pivoting for small ones
   if (A.coarse_n > kCoarseHostMax) {
@@ -837,6 +841,14 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
   }
   A.built = true;
   A.version++;
+  if (dbg) {
+    cudaStreamSynchronize(ctx->st);
+    auto te = std::chrono::steady_clock::now();
+    fprintf(stderr, "amg set-up %.3f ms: levels %.3f ms, coarse inverse (%d unknowns) %.3f ms\n",
+            std::chrono::duration<double, std::milli>(te - ts).count(),
+            std::chrono::duration<double, std::milli>(tl - ts).count(), A.coarse_n,
+            std::chrono::duration<double, std::milli>(te - tl).count());
+  }
   return PFEM_OK;
 }
 
@@ -1069,8 +1081,14 @@ int krylov_inner(pfem_ctx* ctx, int method, double rtol, int itmax, int* iters, 
   *iters = 0;
   *conv = false;
   if (method == PFEM_KRYLOV_CG) {
+    const bool dbg = getenv("PFEM_DEBUG_AMG") != nullptr;
+    auto tg = std::chrono::steady_clock::now();
     int rc = cg_graph_build<T>(ctx);
     if (rc) return rc;
+    if (dbg) {
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tg).count();
+      if (ms > 0.05) fprintf(stderr, "cg graph capture + instantiate %.3f ms\n", ms);
+    }
     CgGraph& G = cg_of<T>(ctx);
     const double ctl[2] = {rtol, (double)std::max(itmax, 1)};
     CK(cudaMemcpyAsync(G.ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
