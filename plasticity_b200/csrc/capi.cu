@@ -467,10 +467,11 @@ void mgs_qr(int m, std::vector<double>& A, double R[36]) {
 // PFEM_COARSE_DENSE_MAX overrides the bound.
 constexpr long long kCoarseDenseMax = 1500;
 // Coarsest levels up to this size are inverted on the host with partial pivoting
-// (n^3 <= 2e8 flops); larger ones on the device without row exchanges, which the
-// coarse operators of large meshes (full aggregates, every rigid mode present)
-// do not need.
-constexpr int kCoarseHostMax = 600;
+// (n^3 <= 2.7e7 multiply-adds: 1.3 ms at 162 unknowns, but 16 ms at 384); larger
+// ones on the device without row exchanges (about 1.4 ms at 384), which the
+// coarse operators of all but the smallest meshes (full aggregates, every rigid
+// mode present) do not need.
+constexpr int kCoarseHostMax = 300;
 
 void build_amg_structure(pfem_ctx* c) {
   long long dense_max = kCoarseDenseMax;
@@ -730,34 +731,39 @@ int krylov_alloc(pfem_ctx* ctx) {
 // elimination can meet tiny pivots: partially constrained aggregates leave
 // coarse rows that are nearly dependent.
 void dense_inverse_host(int n, std::vector<double>& a, std::vector<double>& inv) {
-  inv.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+  // In-place Gauss-Jordan with partial pivoting (n^3 multiply-adds): column c of the
+  // identity is never stored, the pivot row's slot c takes 1 / pivot, and the row
+  // exchanges are undone on the columns at the end.
   double scl = 0;
   for (int i = 0; i < n; ++i) scl = std::max(scl, std::fabs(a[(size_t)i * n + i]));
+  std::vector<int> perm(n);
   for (int c = 0; c < n; ++c) {
     int piv = c;
     double best = std::fabs(a[(size_t)c * n + c]);
     for (int r = c + 1; r < n; ++r)
       if (std::fabs(a[(size_t)r * n + c]) > best) { best = std::fabs(a[(size_t)r * n + c]); piv = r; }
+    perm[c] = piv;
     if (piv != c)
-      for (int j = 0; j < n; ++j) {
-        std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
-        std::swap(inv[(size_t)c * n + j], inv[(size_t)piv * n + j]);
-      }
-    double pv = a[(size_t)c * n + c];
+      for (int j = 0; j < n; ++j) std::swap(a[(size_t)c * n + j], a[(size_t)piv * n + j]);
+    double* rc = a.data() + (size_t)c * n;
+    double pv = rc[c];
     if (std::fabs(pv) < 1e-14 * std::max(scl, 1e-300)) pv = (pv >= 0 ? 1.0 : -1.0) * 1e-14 * std::max(scl, 1e-300);
     const double ip = 1.0 / pv;
-    for (int j = 0; j < n; ++j) { a[(size_t)c * n + j] *= ip; inv[(size_t)c * n + j] *= ip; }
+    rc[c] = 1.0;
+    for (int j = 0; j < n; ++j) rc[j] *= ip;
     for (int r = 0; r < n; ++r) {
       if (r == c) continue;
-      const double f = a[(size_t)r * n + c];
+      double* rr = a.data() + (size_t)r * n;
+      const double f = rr[c];
       if (f == 0.0) continue;
-      for (int j = 0; j < n; ++j) {
-        a[(size_t)r * n + j] -= f * a[(size_t)c * n + j];
-        inv[(size_t)r * n + j] -= f * inv[(size_t)c * n + j];
-      }
+      rr[c] = 0.0;
+      for (int j = 0; j < n; ++j) rr[j] -= f * rc[j];
     }
   }
+  for (int c = n - 1; c >= 0; --c)
+    if (perm[c] != c)
+      for (int i = 0; i < n; ++i) std::swap(a[(size_t)i * n + c], a[(size_t)i * n + perm[c]]);
+  inv.swap(a);
 }
 
 // Numeric AMG set-up on the current (Dirichlet-imposed) tangent of precision T:

@@ -19,7 +19,7 @@ namespace pfem {
 //   3: xo = c2 x + c1 (y - Dinv A x)        (fused degree-2 Chebyshev, x = d0, y = r0)
 //   4: as 3, added to xo
 //   5: y = Dinv (b - A x), xo = c1 y        (preconditioned residual + first direction)
-template <typename T, int BS, int MODE, bool VEC = false>
+template <typename T, int BS, int MODE, bool VEC = false, int LANES = 16>
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __restrict__ rowptr,
                                                        const int* __restrict__ col,
                                                        const T* __restrict__ val,
@@ -27,17 +27,19 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
                                                        const T* __restrict__ b,
                                                        const T* __restrict__ dinv, T* __restrict__ xo,
                                                        T c1, T c2) {
-  // Half a warp per block row (a level-0 row has at most 27 blocks: two per
-  // lane); values and column ids are read once, through the streaming
+  // LANES lanes per block row: half a warp for 3 x 3 blocks (a level-0 row has at
+  // most 27 blocks: two per lane), a warp for 6 x 6 blocks (one 144-byte block
+  // per lane); values and column ids are read once, through the streaming
   // (evict-first) path so they do not push the gathered x out of the caches.
-  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4);
-  const int lane = threadIdx.x & 15;
+  static_assert(LANES == 16 || LANES == 32, "half or whole warps per row");
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) / LANES);
+  const int lane = threadIdx.x & (LANES - 1);
   const bool ok = row < nbrow;
   const int s = ok ? rowptr[row] : 0, e = ok ? rowptr[row + 1] : 0;
   T acc[BS];
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
-  for (int k = s + lane; k < e; k += 16) {
+  for (int k = s + lane; k < e; k += LANES) {
     const int c = __ldcs(col + k);
     const T* B = val + (long long)k * (BS * BS);
     T bv[BS * BS];
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
   for (int i = 0; i < BS; ++i) {
     T v = acc[i];
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     acc[i] = v;
   }
   if (ok && lane < BS) {
@@ -117,16 +119,17 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
 template <typename T, int MODE>
 static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const T* dinv, T* xo, T c1, T c2,
                         cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * 16;
+  const long long threads = (long long)A.nbrow * (A.bs == 3 ? 16 : 32);
   const int blocks = (int)((threads + 255) / 256);
   pfem::count_launch();
   if (A.bs == 3)
     bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
   else if ((reinterpret_cast<uintptr_t>(A.val) & 15) == 0)
-    bsr_spmv_kernel<T, 6, MODE, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1,
-                                                              c2);
+    bsr_spmv_kernel<T, 6, MODE, true, 32><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo,
+                                                                  c1, c2);
   else
-    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+    bsr_spmv_kernel<T, 6, MODE, false, 32><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo,
+                                                                   c1, c2);
 }
 
 template <typename T>
