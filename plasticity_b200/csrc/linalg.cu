@@ -119,17 +119,25 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
 template <typename T, int MODE>
 static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const T* dinv, T* xo, T c1, T c2,
                         cudaStream_t st) {
-  const long long threads = (long long)A.nbrow * (A.bs == 3 ? 16 : 32);
+  // 6 x 6 levels of fewer than kWarpRowsBelow rows fill too few warp slots with half
+  // a warp per row: give each row a whole warp there (measured at 64^3: level 2,
+  // 512 rows, 7.4 -> 6.5 us per pass; level 1, 10,648 rows, 14.3 -> 18.2 us)
+  constexpr int kWarpRowsBelow = 4096;
+  const bool wide = A.bs == 6 && A.nbrow < kWarpRowsBelow;
+  const long long threads = (long long)A.nbrow * (wide ? 32 : 16);
   const int blocks = (int)((threads + 255) / 256);
+  const bool aligned = (reinterpret_cast<uintptr_t>(A.val) & 15) == 0;
   pfem::count_launch();
   if (A.bs == 3)
     bsr_spmv_kernel<T, 3, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
-  else if ((reinterpret_cast<uintptr_t>(A.val) & 15) == 0)
+  else if (aligned && wide)
     bsr_spmv_kernel<T, 6, MODE, true, 32><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo,
                                                                   c1, c2);
+  else if (aligned)
+    bsr_spmv_kernel<T, 6, MODE, true><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1,
+                                                              c2);
   else
-    bsr_spmv_kernel<T, 6, MODE, false, 32><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo,
-                                                                   c1, c2);
+    bsr_spmv_kernel<T, 6, MODE><<<blocks, 256, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
 }
 
 template <typename T>
