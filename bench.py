@@ -164,7 +164,7 @@ def solver_kw(kind, have_mlp):
         return dict(precision="mixed", predictor=learned, line_search=True, amg_rebuild=False)
     if kind == "fp64":
         return dict(precision="fp64", predictor="previous", line_search=True, eta_first=0.0,
-                    amg_rebuild=False)
+                    amg_rebuild=False, ew_need=False)
     if kind == "fp64_extrapolate":
         return dict(precision="fp64", predictor="extrapolate", line_search=True)
     if kind == "truth":

@@ -104,6 +104,10 @@ typedef struct pfem_solve_opts {
                             boundary-value jump), the inner tolerance is capped at eta_first;
                             <= 0 = the reference's forcing term throughout */
   double amg_stale_ratio; /* amg_rebuild = 2 only (default 1.5) */
+  int32_t ew_need;       /* Eisenstat-Walker forcing only: 1 (default) never asks an inner solve
+                            for more than the Newton test needs, eta >= 0.5 tol
+                            max(|R_1|, |F_ext|, 1) / |R_k| (no oversolving in the last
+                            iteration); 0 = the reference's forcing term (Solver.jl:159-171) */
 } pfem_solve_opts;
 
 typedef struct pfem_solve_result {

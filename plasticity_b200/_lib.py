@@ -45,7 +45,7 @@ class SolveOpts(C.Structure):
                 ("ew_alpha", C.c_double), ("krylov_itmax", C.c_int32), ("predictor", C.c_int32),
                 ("amg_rebuild", C.c_int32), ("cheb_degree", C.c_int32), ("verbose", C.c_int32),
                 ("line_search", C.c_int32), ("predictor_smooth", C.c_int32), ("max_cuts", C.c_int32),
-                ("eta_first", C.c_double), ("amg_stale_ratio", C.c_double)]
+                ("eta_first", C.c_double), ("amg_stale_ratio", C.c_double), ("ew_need", C.c_int32)]
 
 
 class SolveResultC(C.Structure):

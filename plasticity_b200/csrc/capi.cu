@@ -1423,6 +1423,10 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     }
     if (it == o->maxiter) break;
     double eta = o->lin_rtol > 0 ? o->lin_rtol : forcing_term(o, it, rn, rkm1, eta_prev);
+    // The step only has to bring |R| under the Newton test: a tighter inner solve in
+    // the last iteration is wasted (Eisenstat-Walker's own safeguard; the reference
+    // has none).  Half the needed reduction leaves room for the linearisation error.
+    if (o->lin_rtol <= 0 && o->ew_need) eta = std::max(eta, std::min(o->eta_max, 0.5 * o->tol * ref / rn));
     // After a backtracked step the iterate is outside Newton's fast region; a
     // loose inner solve there gives poor directions, so tighten it.
     if (damped) eta = std::min(eta, 1e-3);
@@ -1633,6 +1637,7 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->max_cuts = 0;
   o->eta_first = 1e-2;
   o->amg_stale_ratio = 1.5;
+  o->ew_need = 1;
 }
 
 namespace {

@@ -284,7 +284,7 @@ class Model:
     def _opts(self, nsteps=10, tol=1e-8, maxiter=25, precision="fp64", linsolve="cg", lin_rtol=None,
               predictor="previous", amg_rebuild=None, cheb_degree=2, cg_itmax=200, eta_min=None,
               line_search=False, verbose=False, predictor_smooth=None, eta_max=None, max_cuts=0,
-              eta_first=None, amg_stale_ratio=None):
+              eta_first=None, amg_stale_ratio=None, ew_need=None):
         o = L.SolveOpts()
         L.lib().pfem_default_opts(C.byref(o))
         o.nsteps, o.maxiter, o.tol = nsteps, maxiter, tol
@@ -300,6 +300,8 @@ class Model:
             o.amg_rebuild = 2 if amg_rebuild == "adaptive" else int(bool(amg_rebuild))
         if amg_stale_ratio is not None:
             o.amg_stale_ratio = float(amg_stale_ratio)
+        if ew_need is not None:
+            o.ew_need = int(bool(ew_need))
         o.cheb_degree = cheb_degree
         o.krylov_itmax = cg_itmax
         o.verbose = int(bool(verbose))
