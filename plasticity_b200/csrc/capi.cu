@@ -1333,7 +1333,8 @@ int residual_system(pfem_ctx* ctx, int prec, double lam, double* rnorm, double* 
 // Solve K dU = -R (device R) with precision prec; the correction stays in
 // the precision-T Krylov vector kw.x.
 int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool rebuild, int* kits,
-                      double* t_amg, double* t_kry, bool* converged = nullptr) {
+                      double* t_amg, double* t_kry, bool* converged = nullptr, int itmax = -1) {
+  if (itmax <= 0) itmax = o->krylov_itmax;
   const int prec = o->precision;
   int rc;
   auto t0 = std::chrono::steady_clock::now();
@@ -1361,10 +1362,10 @@ int newton_correction(pfem_ctx* ctx, const pfem_solve_opts* o, double rtol, bool
   bool conv = false;
   if (prec == PFEM_FP64) {
     convert<double, double>(ctx->ndof, ctx->dR, ctx->kw64.b, -1.0, ctx->st);
-    rc = krylov<double>(ctx, o->krylov, rtol, o->krylov_itmax, kits, &conv);
+    rc = krylov<double>(ctx, o->krylov, rtol, itmax, kits, &conv);
   } else {
     convert<double, float>(ctx->ndof, ctx->dR, ctx->kw32.b, -1.0, ctx->st);
-    rc = krylov<float>(ctx, o->krylov, rtol, o->krylov_itmax, kits, &conv);
+    rc = krylov<float>(ctx, o->krylov, rtol, itmax, kits, &conv);
   }
   if (rc) return rc;
   CKL();
@@ -1439,7 +1440,15 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     int kits = 0;
     bool kconv = true;
     double amg0 = tm->amg_ms, kry0 = tm->kry_ms;
-    rc = newton_correction(ctx, o, eta, rebuild, &kits, &tm->amg_ms, &tm->kry_ms, &kconv);
+    // A solve on a reused hierarchy that needs far more than its fresh rate is cut
+    // short and redone on a rebuilt one (below), instead of running to convergence
+    // on the stale hierarchy first.
+    int cap = -1;
+    if (o->amg_rebuild == 2 && !rebuild && ctx->amg_ipd_base > 0) {
+      const double expect = ctx->amg_ipd_base * std::max(std::log10(1.0 / eta), 0.5);
+      cap = std::min(o->krylov_itmax, std::max(12, (int)std::ceil(2.0 * (o->amg_stale_ratio * expect + 2))));
+    }
+    rc = newton_correction(ctx, o, eta, rebuild, &kits, &tm->amg_ms, &tm->kry_ms, &kconv, cap);
     if (rc) return rc;
     if (o->amg_rebuild == 2 && !rebuild && !kconv) {
       // a reused hierarchy that no longer reaches the tolerance: rebuild and solve again,
