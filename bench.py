@@ -134,17 +134,22 @@ class Clocks:
                 "sampler": "nvml 10 ms" if self._nv is not None else "nvidia-smi 200 ms"}
 
 
-def ncu_traffic(kernel):
+def ncu_traffic(kernel, algorithmic_bytes):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel`
-    from the committed ncu summary profiles/ncu_traffic.txt, or None."""
+    from the committed ncu summary profiles/ncu_traffic.txt, and how it was obtained.
+    The capture is of the 64^3 launch; for another size the captured traffic is scaled
+    by the ratio of algorithmic bytes (the SpMV's traffic grows in proportion)."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
-        return None
+        return None, None
     for line in open(p):
         f = line.split()
-        if len(f) >= 2 and not line.startswith("#") and f[0] == kernel:
-            return float(f[1])
-    return None
+        if len(f) >= 3 and not line.startswith("#") and f[0] == kernel:
+            t, alg = float(f[1]), float(f[2])
+            if abs(algorithmic_bytes - alg) <= 1e-6 * alg:
+                return t, "ncu capture of this launch (profiles/ncu_traffic.txt)"
+            return t * algorithmic_bytes / alg, "64^3 ncu capture scaled by algorithmic bytes"
+    return None, None
 
 
 def spmv_bytes(nnzb, nbrow, bs, vbytes):
@@ -390,13 +395,14 @@ def main():
         nnzb = M.pattern()[1].size // 9
         by = spmv_bytes(nnzb, M.nn, 3, 4)
         achieved = by / (spmv_ms * 1e-3) / 1e9
+        traffic, traffic_src = ncu_traffic("bsr_spmv_kernel<float,3,0>", by)
         return {"kernel": "bsr_spmv_kernel<float,3> (level-0 tangent SpMV, FP32 values)", "bound": "hbm",
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                 "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if pk_kind == "measured"
                                 else "fallback 6,650 GB/s (no MEASURED_PEAKS.json on this box)"),
                 "algorithmic_bytes_per_launch": by, "avg_launch_ms": spmv_ms,
                 "timing": "20 back-to-back launches on the library stream, CUDA events, after the timed region",
-                "traffic": ncu_traffic("bsr_spmv_kernel<float,3,0>"),
+                "traffic": traffic, "traffic_source": traffic_src,
                 "element_assembly_ms": asm_ms}
     roof = guarded("roofline", roofline)
     del M
