@@ -696,7 +696,6 @@ int amg_alloc(pfem_ctx* ctx) {
     CK(dalloc(ctx, &v.x, n)); CK(dalloc(ctx, &v.b, n)); CK(dalloc(ctx, &v.r, n));
     CK(dalloc(ctx, &v.d, n)); CK(dalloc(ctx, &v.t, n));
     if (l >= 2) { CK(dalloc(ctx, &v.b2, n)); CK(dalloc(ctx, &v.x2, n)); }
-    CK(dalloc(ctx, &v.ev, n));
   }
   const HostLevel& hc = ctx->hl[L];
   A.coarse_n = hc.nbrow * hc.bs;
@@ -789,31 +788,20 @@ int amg_setup(pfem_ctx* ctx, int cheb_degree) {
     AmgLevel<T>& v = A.lv[l];
     blockdiag_invert<T>(v.A, v.dinv, ctx->st);
     CKL();
-    // power iteration on D^-1 A: 12 steps from a fixed pseudo-random vector on the
-    // first set-up, 5 from the previous set-up's vector afterwards (the operator
-    // changes little between rebuilds, and the warm start is closer to converged
-    // than 12 cold steps)
+    // power iteration on D^-1 A
     const long long n = (long long)v.A.nbrow * v.A.bs;
-    const bool warm = v.ev_valid;
-    if (warm) {
-      CK(cudaMemcpyAsync(v.d, v.ev, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
-    } else {
-      pfem::count_launch();
-      hash_fill_kernel<<<256, 256, 0, ctx->st>>>(n, std::is_same<T, float>::value ? (float*)v.d : nullptr,
-                                                 std::is_same<T, double>::value ? (double*)v.d : nullptr);
-    }
-    for (int it = 0; it < (warm ? 5 : 12); ++it) {
+    pfem::count_launch(); hash_fill_kernel<<<256, 256, 0, ctx->st>>>(n, std::is_same<T, float>::value ? (float*)v.d : nullptr,
+                                               std::is_same<T, double>::value ? (double*)v.d : nullptr);
+    for (int it = 0; it < 12; ++it) {
       bsr_spmv<T>(v.A, v.d, v.t, ctx->st);
       blockdiag_apply<T>(v.A.nbrow, v.A.bs, v.dinv, v.t, v.r, T(1), nullptr, ctx->st);
       dot<T>(n, v.r, v.r, w.sc + 8, w.part, ctx->st, true);
       pfem::count_launch(); scale_by_inv_kernel<T><<<256, 256, 0, ctx->st>>>(n, w.sc + 8, v.r, v.d);
     }
     CKL();
-    CK(cudaMemcpyAsync(v.ev, v.d, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->st));
     T lm = 0;
     CK(cudaMemcpyAsync(&lm, w.sc + 8, sizeof(T), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    v.ev_valid = std::isfinite((double)lm) && lm > 0;  // a broken estimate never seeds the next one
     v.lmax = (T)(1.1 * (double)lm);
     if (getenv("PFEM_DEBUG_AMG"))
       fprintf(stderr, "amg level %d: block rows %d bs %d nnzb %lld aggregates %d P blocks %d lmax %.4g\n", l,

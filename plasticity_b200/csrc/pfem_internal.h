@@ -100,9 +100,6 @@ struct AmgLevel {
   VT *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
   // second coarse iteration of a W-cycle visit (levels >= 2): its right-hand side and result
   VT *b2 = nullptr, *x2 = nullptr;
-  // the last power iteration's normalised vector: the next set-up starts from it
-  VT* ev = nullptr;
-  bool ev_valid = false;
 };
 
 template <typename VT>
