@@ -238,7 +238,9 @@ int pfem_gauss_stress(const pfem_ctx* ctx, double* sigma);
 /* Device timing of one hot-path kernel family on the resident data, CUDA
  * events on the context's stream, averaged over reps launches.
  * what: 0 = element kernels of one full assembly (all colors, FP64 tangent),
- *       1 = same with the FP32 tangent, 2 = level-0 SpMV FP32, 3 = SpMV FP64. */
+ *       1 = same with the FP32 tangent, 2 = level-0 SpMV FP32, 3 = SpMV FP64,
+ *       4 = one cycle of the resident FP32 AMG hierarchy, captured once in a CUDA
+ *           graph and replayed (as inside the CG loop). */
 int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms_per_launch);
 
 /* CUDA-event timer on the context's stream (the stream every kernel of this

@@ -2703,6 +2703,37 @@ int pfem_profile(pfem_ctx* ctx, int32_t what, int32_t reps, double* ms) {
       for (int i = 0; i < reps; ++i) bsr_spmv<double>(A, ctx->kw64.p, ctx->kw64.q, ctx->st);
       CK(cudaEventRecord(ctx->e1, ctx->st));
     }
+  } else if (what == 4) {
+    // one cycle of the resident FP32 hierarchy as it runs inside the CG loop: captured
+    // once into a CUDA graph, replayed reps times
+    if (!ctx->amg32.built) return fail(ctx, PFEM_ERR_STATE, "no FP32 AMG hierarchy built");
+    KrylovWork<float>& w = ctx->kw32;
+    fill<float>(ctx->ndof, w.r, 1.0f, ctx->st);
+    CK(cudaStreamSynchronize(ctx->st));
+    const long long c0 = pfem::launch_counter();
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+    vcycle<float>(ctx, 0, w.r, w.z);
+    cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+    pfem::launch_counter() = c0;  // counted when replayed below, not when captured
+    if (e != cudaSuccess) return fail(ctx, PFEM_ERR_CUDA, std::string("cycle capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ge, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return fail(ctx, PFEM_ERR_CUDA, std::string("cycle graph instantiate: ") + cudaGetErrorString(e));
+    }
+    size_t nodes = 0;
+    cudaGraphGetNodes(g, nullptr, &nodes);
+    e = cudaGraphLaunch(ge, ctx->st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->e0, ctx->st);
+    for (int i = 0; i < reps && e == cudaSuccess; ++i) e = cudaGraphLaunch(ge, ctx->st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->e1, ctx->st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ctx->e1);
+    pfem::launch_counter() += (long long)nodes * (reps + 1);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(ctx, PFEM_ERR_CUDA, std::string("cycle graph replay: ") + cudaGetErrorString(e));
   } else {
     return PFEM_ERR_BAD_ARG;
   }

@@ -104,6 +104,7 @@ def main():
         for _ in range(args.reps):
             M.amg_apply(-R)
         out["amg_cycle_host_ms"] = (time.perf_counter() - t0) * 1e3 / args.reps
+        out["amg_cycle_graph_ms"] = M.profile(4, reps=20)
     if "residual" in what:
         t0 = time.perf_counter()
         for _ in range(args.reps):
