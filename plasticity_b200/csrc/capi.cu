@@ -81,6 +81,8 @@ struct pfem_ctx {
   std::string err;
   std::vector<void*> allocs;
   std::vector<int> bc_dofs;    // deduplicated Dirichlet dofs of the last pfem_set_bcs
+  std::vector<int64_t> neu_dofs_last;  // the Neumann arrays of the last pfem_set_bcs, as given
+  std::vector<double> neu_vals_last;
 
   // host topology
   std::vector<double> X;        // nn*3
@@ -2006,33 +2008,39 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   if (ctx->device < 0) return fail(ctx, PFEM_ERR_STATE, "topology-only context (device < 0)");
   cudaSetDevice(ctx->device);
   const long long ndof = ctx->ndof;
-  // _freeze_bcs: last assignment wins (Solver.jl:192-218)
-  std::vector<int> last(ndof, -1);
-  for (int64_t i = 0; i < ndir; ++i) {
-    const int64_t d = dir_dofs[i] - 1;
-    if (d < 0 || d >= ndof) return fail(ctx, PFEM_ERR_BAD_ARG, "Dirichlet dof out of range");
-    last[d] = (int)i;
-  }
+  // _freeze_bcs: last assignment wins (Solver.jl:192-218).  The entries are ordered
+  // by dof (a stable sort keeps a dof's assignments in call order) and the last of
+  // each run is kept: host work in the number of constraints, not of dofs, so that
+  // per-increment updates stay cheap.
+  for (int64_t i = 0; i < ndir; ++i)
+    if (dir_dofs[i] < 1 || dir_dofs[i] > ndof) return fail(ctx, PFEM_ERR_BAD_ARG, "Dirichlet dof out of range");
+  for (int64_t i = 0; i < nneu; ++i)
+    if (neu_dofs[i] < 1 || neu_dofs[i] > ndof) return fail(ctx, PFEM_ERR_BAD_ARG, "Neumann dof out of range");
+  std::vector<int64_t> order((size_t)ndir);
+  for (int64_t i = 0; i < ndir; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t c) { return dir_dofs[a] < dir_dofs[c]; });
   std::vector<int> dofs;
   std::vector<double> vals;
   std::vector<uint8_t> ramp;
-  std::vector<uint8_t> isbc(ndof, 0);
-  for (long long d = 0; d < ndof; ++d)
-    if (last[d] >= 0) {
-      dofs.push_back((int)d);
-      vals.push_back(dir_vals[last[d]]);
-      ramp.push_back(dir_ramp ? dir_ramp[last[d]] : 1);
-      isbc[d] = 1;
-    }
-  std::vector<double> fn(ndof, 0.0);
-  for (int64_t i = 0; i < nneu; ++i) {
-    const int64_t d = neu_dofs[i] - 1;
-    if (d < 0 || d >= ndof) return fail(ctx, PFEM_ERR_BAD_ARG, "Neumann dof out of range");
-    fn[d] += neu_vals[i];
+  for (int64_t k = 0; k < ndir; ++k) {
+    const int64_t i = order[k];
+    if (k + 1 < ndir && dir_dofs[order[k + 1]] == dir_dofs[i]) continue;  // a later assignment follows
+    dofs.push_back((int)(dir_dofs[i] - 1));
+    vals.push_back(dir_vals[i]);
+    ramp.push_back(dir_ramp ? dir_ramp[i] : 1);
   }
-  double s = 0;
-  for (double v : fn) s += v * v;
-  ctx->fn_norm = std::sqrt(s);
+  // the Neumann load vector is rebuilt (an O(ndof) pass and upload) only when it changed
+  const bool same_neu = ctx->bcs_set && (size_t)nneu == ctx->neu_dofs_last.size() &&
+                        std::equal(neu_dofs, neu_dofs + nneu, ctx->neu_dofs_last.begin()) &&
+                        std::equal(neu_vals, neu_vals + nneu, ctx->neu_vals_last.begin());
+  std::vector<double> fn;
+  if (!same_neu) {
+    fn.assign(ndof, 0.0);
+    for (int64_t i = 0; i < nneu; ++i) fn[neu_dofs[i] - 1] += neu_vals[i];
+    double s = 0;
+    for (double v : fn) s += v * v;
+    ctx->fn_norm = std::sqrt(s);
+  }
   BcDev& b = ctx->bc;
   if (ctx->bcs_set && dofs == ctx->bc_dofs) {
     // same constrained dofs: the imposition lists stand, only values change
@@ -2042,10 +2050,20 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
     CK(cudaStreamSynchronize(ctx->st));
     CK(h2d(ctx, b.vals, vals.data(), vals.size() * sizeof(double)));
     CK(h2d(ctx, b.ramp, ramp.data(), ramp.size() * sizeof(uint8_t)));
-    CK(h2d(ctx, b.fn, fn.data(), fn.size() * sizeof(double)));
+    if (!same_neu) {
+      CK(h2d(ctx, b.fn, fn.data(), fn.size() * sizeof(double)));
+      ctx->neu_dofs_last.assign(neu_dofs, neu_dofs + nneu);
+      ctx->neu_vals_last.assign(neu_vals, neu_vals + nneu);
+    }
     ctx->bcs_set = true;
     return PFEM_OK;
   }
+  if (same_neu) {  // the constrained set changed but the loads did not: rebuild fn for the upload below
+    fn.assign(ndof, 0.0);
+    for (int64_t i = 0; i < nneu; ++i) fn[neu_dofs[i] - 1] += neu_vals[i];
+  }
+  std::vector<uint8_t> isbc(ndof, 0);
+  for (int d : dofs) isbc[d] = 1;
   // entries touched by the imposition
   auto blk = [&](int n, int m) -> long long {
     const int* b0 = ctx->bcol.data() + ctx->browptr[n];
@@ -2109,6 +2127,8 @@ int pfem_set_bcs(pfem_ctx* ctx, const int64_t* dir_dofs, const double* dir_vals,
   CK(upload(ctx, &b.zpos, zpos));
   CK(upload(ctx, &b.zone, zone));
   ctx->bc_dofs = dofs;
+  ctx->neu_dofs_last.assign(neu_dofs, neu_dofs + nneu);
+  ctx->neu_vals_last.assign(neu_vals, neu_vals + nneu);
   ctx->bcs_set = true;
   ctx->amg_stale = true;  // a new constrained set changes the imposed tangent's structure
   return PFEM_OK;

@@ -320,3 +320,36 @@ def test_gathered_assembly_matches_colored(precision, monkeypatch):
     assert abs(Kg - Kc).max() <= tolk * abs(Kc).max()
     assert np.linalg.norm(Rg - Rc) <= 1e-13 * np.linalg.norm(Rc)
     assert np.array_equal(tg, tc) and np.array_equal(fg, fc)
+
+
+def test_boundary_condition_update_semantics():
+    """What the cheap same-dofs path of pfem_set_bcs must keep: a Dirichlet dof given
+    twice takes its last value (_freeze_bcs, Solver.jl:192-218), and Neumann loads
+    changed on a reused model act as on a fresh model (bit for bit)."""
+    w = W.config0(n=3, nsteps=2)
+    U = 1e-3 * np.random.default_rng(3).standard_normal(3 * w.mesh.nnodes)
+
+    def residual(dd, dv, dr, nd, nv, M=None):
+        if M is None:
+            M = P.Model(w.mesh, P.J2Material(**w.material))
+        M.dir_dofs, M.dir_vals, M.dir_ramp = dd, dv, dr
+        M.neu_dofs, M.neu_vals = nd, nv
+        M._bcs_dirty = True
+        M.set_displacement(U)
+        return M, M.residual(0.5)[1]
+
+    d, v, r = w.dir_dofs, w.dir_vals, w.dir_ramp
+    top = r == 1
+    dd = np.concatenate([d[top], d])                       # the top dofs first at 0.02, then their own values
+    dv = np.concatenate([np.full(int(top.sum()), 0.02), v])
+    dr = np.concatenate([r[top], r])
+    none_i, none_v = np.zeros(0, np.int64), np.zeros(0)
+    _, Ra = residual(dd, dv, dr, none_i, none_v)
+    _, Rb = residual(d, v, r, none_i, none_v)
+    assert np.array_equal(Ra, Rb)
+    nd = d[top][:5] - 2                                    # free x dofs of top-face nodes
+    M, _ = residual(d, v, r, nd, np.full(5, 1.0))
+    M, R2 = residual(d, v, r, nd, np.full(5, 3.0), M)       # same dofs, new loads: the cheap path
+    _, R3 = residual(d, v, r, nd, np.full(5, 3.0))
+    assert np.array_equal(R2, R3)
+    assert not np.array_equal(R2, residual(d, v, r, none_i, none_v)[1])  # the loads do act
