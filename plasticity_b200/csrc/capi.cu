@@ -1644,7 +1644,7 @@ void pfem_default_opts(pfem_solve_opts* o) {
   o->cheb_degree = 2;
   o->verbose = 0;
   o->line_search = 0;
-  o->predictor_smooth = 16;
+  o->predictor_smooth = 8;  // whole 40-increment path at 64^3: 1.37 s (8), 1.40 s (16), 1.50 s (0)
   o->max_cuts = 0;
   o->eta_first = 1e-2;
   o->amg_stale_ratio = 1.5;
