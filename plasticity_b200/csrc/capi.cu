@@ -145,7 +145,7 @@ struct pfem_ctx {
   double amg_ipd_base = -1.0;
   bool amg_stale = true;
   double amg_excess = 0.0;      // Krylov iterations above the fresh rate since the last rebuild
-  double amg_cost_iters = 0.0;  // the last rebuild's time in Krylov iterations of its hierarchy
+  double amg_cost_iters = 0.0;  // what a rebuild costs, in Krylov iterations
   double lam_prev = 0.0, lam_prev2 = 0.0, lam_prev3 = 0.0;
 };
 
@@ -473,6 +473,8 @@ constexpr long long kCoarseDenseMax = 1500;
 // ones on the device without row exchanges (about 1.4 ms at 384), which the
 // coarse operators of all but the smallest meshes (full aggregates, every rigid
 // mode present) do not need.
+// The adaptive AMG policy charges a rebuild this many Krylov iterations.
+constexpr double kRebuildCostIters = 12.0;
 constexpr int kCoarseHostMax = 300;
 
 void build_amg_structure(pfem_ctx* c) {
@@ -1441,7 +1443,6 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
     first = false;
     int kits = 0;
     bool kconv = true;
-    double amg0 = tm->amg_ms, kry0 = tm->kry_ms;
     // A solve on a reused hierarchy that needs far more than its fresh rate is cut
     // short and redone on a rebuilt one (below), instead of running to convergence
     // on the stale hierarchy first.
@@ -1457,8 +1458,6 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
       // so the adaptive policy never takes a worse direction than the per-step rebuild
       tm->kits += kits;
       rebuild = true;
-      amg0 = tm->amg_ms;
-      kry0 = tm->kry_ms;
       rc = newton_correction(ctx, o, eta, true, &kits, &tm->amg_ms, &tm->kry_ms, &kconv);
       if (rc) return rc;
     }
@@ -1470,9 +1469,11 @@ int newton_dev(pfem_ctx* ctx, double lam, const pfem_solve_opts* o, int* iters, 
         ctx->amg_ipd_base = ipd;
         ctx->amg_stale = false;
         ctx->amg_excess = 0.0;
-        // what a rebuild costs, in Krylov iterations on the fresh hierarchy
-        const double t_it = kits > 0 ? (tm->kry_ms - kry0) / kits : 0.0;
-        ctx->amg_cost_iters = t_it > 0.0 ? (tm->amg_ms - amg0) / t_it : 0.0;
+        // what a rebuild costs, in Krylov iterations on the fresh hierarchy: a fixed
+        // count, so that the policy's decisions (and the solution) do not depend on
+        // timings (measured: set-up plus the CG graph's capture over one PCG iteration
+        // is about 13 at 64^3 and 10 at 100^3)
+        ctx->amg_cost_iters = kRebuildCostIters;
       } else {
         // stale when one solve needs amg_stale_ratio times the fresh rate, or when the
         // iterations spent above the fresh rate since the rebuild have cost more than
