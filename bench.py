@@ -152,10 +152,10 @@ def ncu_traffic(kernel, algorithmic_bytes):
     return None, None
 
 
-def spmv_bytes(nnzb, nbrow, bs, vbytes):
-    """Algorithmic bytes of one block-CSR SpMV: values + block column ids +
-    row pointers + x read once + y written once."""
-    return nnzb * bs * bs * vbytes + nnzb * 4 + (nbrow + 1) * 4 + 2 * nbrow * bs * vbytes
+def spmv_bytes(nnzb, nbrow, bs, vbytes, ibytes=4):
+    """Algorithmic bytes of one block-CSR SpMV: values + block column ids (ibytes
+    each) + row pointers + x read once + y written once."""
+    return nnzb * bs * bs * vbytes + nnzb * ibytes + (nbrow + 1) * 4 + 2 * nbrow * bs * vbytes
 
 
 def solver_kw(kind, have_mlp):
@@ -393,7 +393,7 @@ def main():
         spmv_ms = M.profile(2, reps=20)
         asm_ms = M.profile(1, reps=3)
         nnzb = M.pattern()[1].size // 9
-        by = spmv_bytes(nnzb, M.nn, 3, 4)
+        by = spmv_bytes(nnzb, M.nn, 3, 4, M.tangent_index_bytes())
         achieved = by / (spmv_ms * 1e-3) / 1e9
         traffic, traffic_src = ncu_traffic("bsr_spmv_kernel<float,3,0>", by)
         return {"kernel": "bsr_spmv_kernel<float,3> (level-0 tangent SpMV, FP32 values)", "bound": "hbm",

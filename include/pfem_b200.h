@@ -296,6 +296,12 @@ int pfem_mlp_train(pfem_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t pfem_kernel_launches(void);
 
+/* Bytes per block column index that the level-0 SpMV reads (inspection; no
+ * counterpart in the reference): 2 when every column id of the tangent lies
+ * within +-32767 of its row (offsets stored in 16 bits; node-ordered meshes up to
+ * about 180^3), else 4. */
+int pfem_tangent_index_bytes(pfem_ctx* ctx, int32_t* bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,7 @@ SIGNATURES = {
     "pfem_profile": (C.c_int, [_ctx, C.c_int32, C.c_int32, _d]),
     "pfem_timer": (C.c_int, [_ctx, C.c_int32, _d]),
     "pfem_kernel_launches": (C.c_int64, []),
+    "pfem_tangent_index_bytes": (C.c_int, [_ctx, _i32]),
     "pfem_mlp_init": (C.c_int, [_ctx, C.c_uint64]),
     "pfem_mlp_params": (C.c_int, [_ctx, C.c_int32, _f, C.c_int64]),
     "pfem_mlp_forward": (C.c_int, [_ctx, _f, C.c_int64, _f]),

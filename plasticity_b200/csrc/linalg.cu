@@ -19,9 +19,10 @@ namespace pfem {
 //   3: xo = c2 x + c1 (y - Dinv A x)        (fused degree-2 Chebyshev, x = d0, y = r0)
 //   4: as 3, added to xo
 //   5: y = Dinv (b - A x), xo = c1 y        (preconditioned residual + first direction)
-template <typename T, int BS, int MODE, bool VEC = false, int LANES = 16>
+template <typename T, int BS, int MODE, bool VEC = false, int LANES = 16, bool C16 = false>
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __restrict__ rowptr,
                                                        const int* __restrict__ col,
+                                                       const int16_t* __restrict__ col16,
                                                        const T* __restrict__ val,
                                                        const T* __restrict__ x, T* __restrict__ y,
                                                        const T* __restrict__ b,
@@ -40,7 +41,7 @@ __global__ void __launch_bounds__(256) bsr_spmv_kernel(int nbrow, const int* __r
 #pragma unroll
   for (int i = 0; i < BS; ++i) acc[i] = T(0);
   for (int k = s + lane; k < e; k += LANES) {
-    const int c = __ldcs(col + k);
+    const int c = C16 ? row + (int)__ldcs(col16 + k) : __ldcs(col + k);
     const T* B = val + (long long)k * (BS * BS);
     T bv[BS * BS];
     if constexpr (VEC) {
@@ -131,16 +132,19 @@ static void spmv_launch(const BsrMat<T>& A, const T* x, T* y, const T* b, const 
   const int blocks = (int)((threads + kThreads - 1) / kThreads);
   const bool aligned = (reinterpret_cast<uintptr_t>(A.val) & 15) == 0;
   pfem::count_launch();
-  if (A.bs == 3)
-    bsr_spmv_kernel<T, 3, MODE><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+  if (A.bs == 3 && A.col16)
+    bsr_spmv_kernel<T, 3, MODE, false, 16, true><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.col16,
+                                                                              A.val, x, y, b, dinv, xo, c1, c2);
+  else if (A.bs == 3)
+    bsr_spmv_kernel<T, 3, MODE><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.col16, A.val, x, y, b, dinv, xo, c1, c2);
   else if (aligned && wide)
-    bsr_spmv_kernel<T, 6, MODE, true, 32><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo,
+    bsr_spmv_kernel<T, 6, MODE, true, 32><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.col16, A.val, x, y, b, dinv, xo,
                                                                   c1, c2);
   else if (aligned)
-    bsr_spmv_kernel<T, 6, MODE, true><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1,
+    bsr_spmv_kernel<T, 6, MODE, true><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.col16, A.val, x, y, b, dinv, xo, c1,
                                                               c2);
   else
-    bsr_spmv_kernel<T, 6, MODE><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.val, x, y, b, dinv, xo, c1, c2);
+    bsr_spmv_kernel<T, 6, MODE><<<blocks, kThreads, 0, st>>>(A.nbrow, A.rowptr, A.col, A.col16, A.val, x, y, b, dinv, xo, c1, c2);
 }
 
 template <typename T>

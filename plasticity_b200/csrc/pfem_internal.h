@@ -70,6 +70,9 @@ struct BsrMat {
   int* rowptr = nullptr;  // device, nbrow+1
   int* col = nullptr;     // device, nnzb
   VT* val = nullptr;      // device, nnzb*bs*bs (row-major blocks)
+  // optional, device: col[k] - row as 16-bit offsets (set when every offset fits),
+  // read by the SpMV in place of col
+  const int16_t* col16 = nullptr;
 };
 
 // One level of smoothed-aggregation AMG.  Every fine block row n belongs to

@@ -484,6 +484,12 @@ class Model:
               self._ctx)
         return losses
 
+    def tangent_index_bytes(self) -> int:
+        """Bytes per block column index the level-0 SpMV reads (2 or 4)."""
+        b = C.c_int32()
+        check(L.lib().pfem_tangent_index_bytes(self._ctx, C.byref(b)), self._ctx)
+        return b.value
+
     def profile(self, what: int, reps: int = 10) -> float:
         ms = C.c_double()
         check(L.lib().pfem_profile(self._ctx, what, reps, C.byref(ms)), self._ctx)

@@ -96,3 +96,15 @@ def test_cycle_timed_in_a_graph():
     ms = M.profile(4, reps=3)
     assert ms > 0
     assert np.array_equal(M.amg_apply(r), z)
+
+
+def test_sixteen_bit_column_offsets():
+    """A node-ordered box mesh's block columns lie within 16-bit offsets of their row,
+    so the level-0 SpMV reads 2-byte indices; its product equals the tangent's
+    (the level-0 operator the cycle and CG use) applied on the host."""
+    M, R = _model(10, "fp64")
+    assert M.tangent_index_bytes() == 2
+    M.linear_solve(-R, rtol=1e-8, rebuild=True, precision="fp64")
+    A0 = M.amg_dense(0, 0)
+    x, its = M.linear_solve(-R, rtol=1e-8, rebuild=False, precision="fp64")
+    assert np.linalg.norm(A0 @ x + R) <= 1e-7 * np.linalg.norm(R)
